@@ -1,0 +1,298 @@
+#!/usr/bin/env python
+"""Swap-evaluation throughput of the SRO-targeted swap search on B200.
+
+Workload (default): the plain GPU configuration -- BCC 20x20x20 (16000 sites,
+8/6/12 shells), 5 species x 3200 atoms, seeded synthetic target alpha
+(U(-0.15, 0.15), zero row sums), weights [4, 1, 0.5], 256 solutions x 512
+tasks, 50 iterations, converge depth 20.  One step = one whole search
+(pyhea/cpp/accelerate.cu:1112-1242 semantics) with a fresh seed.
+
+  value  swap evaluations per second over the K timed steps, device time (CUDA
+         events on the search's stream), inputs resident; summed over ranks and
+         divided by the slowest rank's time
+  e2e    the same metric through the C ABI with host buffers
+         (hea_run_local_parallel_hcs): neighbour table and inputs copied from
+         pinned memory and the population read back inside the timed region
+  roofline  the local-search kernel: algorithmic bytes (2 sum Z (4 B id + 1 B
+         species) + 2 B per evaluation) over its CUDA-event time, against the
+         measured HBM copy bandwidth
+  cpu_baseline  the reference CPU engine (oracle/_ref) on a bounded sample
+
+--impl reference times the reference CPU engine alone (rank 0) on the same
+workload and prints the same line with "impl": "reference".
+Multi-GPU: replicas -- every rank searches its own copy of the workload with
+its own seeds; no collective on the data path.
+"""
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["plain_gpu", "plain_cpu"], default="plain_gpu")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-procs", type=int, default=0, help="reference processes (0: all host cores)")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def workload(name):
+    from pyhea_b200 import workloads as W
+
+    return W.plain_gpu(seed=0) if name == "plain_gpu" else W.plain_cpu(seed=0)
+
+
+def config_of(st, name):
+    return {"workload": f"{name}: {st.name}", "lattice": "FCC" if st.lattice == 0 else "BCC", "cell": st.cell,
+            "sites": st.num_sites, "species": [int(x) for x in st.species],
+            "shells": [len(v) for v in st.shell_sizes()][: len(st.weight)], "weights": [float(w) for w in st.weight],
+            "solutions": st.P, "parallel_task": st.Q, "total_iter": st.I, "converge_depth": st.D,
+            "l2": "flushed between timed steps (256 MiB write)", "step": "one whole search, fresh seed"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower().startswith("active")})
+        loaded = [r[0] for r in rows if r[0] > 0.5 * r[1]] or [r[0] for r in rows]
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_reference_sample(st, nbor, sizes, procs, nnet_per_proc=5, step=1):
+    from oracle.ref_timing import RefPool, available
+
+    if not available():
+        return None
+    pool = RefPool(procs)
+    try:
+        r = pool.sample(nbor, sizes[: len(st.weight)], st.species, st.weight, st.target, nnet_per_proc, step, st.Q,
+                        st.D)
+    finally:
+        pool.close()
+    r["procs"] = procs
+    r["sample"] = (f"{procs} processes x {nnet_per_proc} solutions x {step} iteration(s) of the same structure, "
+                   f"task={st.Q}, depth={st.D}; evaluations from rand() calls x (1 - sum c^2)")
+    return r
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    st = workload(args.workload)
+    nbor, sizes = st.neighbors()
+    procs = args.cpu_procs or host_cores()
+    from oracle.ref_timing import RefPool, available
+
+    if not available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_accelerate.so was not built"}))
+        return 0
+    pool = RefPool(procs)
+    nnet = max(1, 2)
+    total_evals, total_s = 0.0, 0.0
+    try:
+        for i in range(args.warmup + args.steps):
+            r = pool.sample(nbor, sizes[: len(st.weight)], st.species, st.weight, st.target, nnet, 1, st.Q, st.D)
+            if i >= args.warmup:
+                total_evals += r["evals"]
+                total_s += r["wall_s"]
+    finally:
+        pool.close()
+    value = total_evals / total_s
+    sample = (f"per step: {procs} single-rank processes x {nnet} solutions x 1 iteration of the full structure, "
+              f"task={st.Q}, depth={st.D}; evaluations = rand() calls / 2 x (1 - sum c^2)")
+    line = {"metric": "swap_evals_per_sec", "value": value, "unit": "swap-evals/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * total_s / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(st, args.workload),
+            "cpu_baseline": {"value": value, "unit": "swap-evals/s", "cores": procs, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "swap-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    import pyhea_b200 as hb
+
+    st = workload(args.workload)
+    problem = st.problem(device=True)
+    nbor, sizes = st.neighbors(device=True)
+    plan = hb.Plan(problem, st.P, st.I, st.Q, st.D, time_kernels=True)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    base = 1_000_003 * rank
+
+    for w in range(args.warmup):
+        plan.run(base + w)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    total_ms, evals, mc_ms, launches, accepts = 0.0, 0, 0.0, 0, 0
+    for k in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        s = plan.run(base + args.warmup + k)
+        total_ms += s["gpu_ms"]
+        evals += s["evals"]
+        mc_ms += s["mc_ms"]
+        launches += s["mc_launches"]
+        accepts += s["accepts"]
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    _, best = plan.read()
+    plan.close()
+
+    # end to end through the C ABI with pinned host buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    hp = hb.Problem(pin(problem.nbor), pin(problem.shell_sizes), pin(problem.species), pin(problem.weight),
+                    pin(problem.target_sro))
+    out_occ = torch.empty((st.P, st.num_sites), dtype=torch.uint8).pin_memory().numpy()
+    out_fit = torch.empty(st.P, dtype=torch.float64).pin_memory().numpy()
+    e2e_s, e2e_evals = 0.0, 0
+    for k in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, _, s = hb.search(hp, st.P, st.I, st.Q, st.D, seed=base + 7_777 + k, out_occ=out_occ, out_fitness=out_fit)
+        e2e_s += time.perf_counter() - t0
+        e2e_evals += s["evals"]
+    h2d = (hp.nbor.nbytes + hp.shell_sizes.nbytes + hp.species.nbytes + hp.weight.nbytes + hp.target_sro.nbytes)
+    d2h = out_occ.nbytes + out_fit.nbytes
+
+    if dist:
+        t = torch.tensor([total_ms, float(evals), e2e_s, float(e2e_evals)], dtype=torch.float64, device="cuda")
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        total_ms_max, evals_all, e2e_max, e2e_evals_all = tmax[0].item(), t[1].item(), tmax[2].item(), t[3].item()
+    else:
+        total_ms_max, evals_all, e2e_max, e2e_evals_all = total_ms, float(evals), e2e_s, float(e2e_evals)
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        B = st.evals_bytes()
+        achieved = evals * B / (mc_ms / 1000.0) / 1e9 if mc_ms > 0 else None
+        line = {
+            "metric": "swap_evals_per_sec", "value": evals_all / (total_ms_max / 1000.0), "unit": "swap-evals/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(config_of(st, args.workload), parallelism=f"replicas x{world}"),
+            "gpu_launches": None,
+            "e2e": {"value": e2e_evals_all / e2e_max, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "kernel": "mc_kernel (local search)", "bytes_per_eval": B, "peak_kind": peak_kind,
+                         "kernel_share": mc_ms / total_ms if total_ms else None},
+            "search": {"evals_per_step": evals / args.steps, "accepts_per_step": accepts / args.steps,
+                       "best_fitness_last_step": float(best[0])},
+            "clocks": clocks,
+        }
+        # kernels launched per search: 1 generate + per iteration (generate, search, merge, search, sort), plus
+        # the iota of the slot order
+        line["gpu_launches"] = args.steps * (2 + 5 * st.I)
+        if world == 1 and not args.no_cpu_baseline:
+            r = cpu_reference_sample(st, nbor, sizes, args.cpu_procs or host_cores())
+            if r:
+                line["cpu_baseline"] = {"value": r["evals"] / r["wall_s"], "unit": "swap-evals/s", "cores": r["procs"],
+                                        "kind": "reference", "sample": r["sample"]}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,144 @@
+/*
+ * hea_cuda.h -- C ABI of the B200 swap-search engine (libhea_cuda.so).
+ *
+ * The engine replaces the GPU engine of PyHEA, i.e. the function bound by
+ * pyhea/cpp/bind.cpp:49-58 as accelerate.run_local_parallel_hcs_cuda and
+ * declared at pyhea/cpp/accelerate.h:51-60 (implemented at
+ * pyhea/cpp/accelerate.cu:1112-1242).  All pointers here are plain host
+ * pointers; the library owns every device buffer it uses.  No call exits the
+ * process: each returns HEA_OK or an error code, and hea_last_error() gives the
+ * message of the calling thread's last failure.
+ *
+ * Neighbour table layout (the flattened form of pyhea/lattice/lattice.py:
+ * 196-323 output, cut to the first num_shells shells as accelerate.cu:1139-1141
+ * does): nbor[s * row + off_k + q] is the q-th neighbour of site s in shell k,
+ * row = sum of shell_sizes, off_k = sum of the sizes before k.
+ */
+#ifndef HEA_CUDA_H
+#define HEA_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HEA_OK 0
+#define HEA_ERR_INVALID 1     /* an argument is out of range or inconsistent      */
+#define HEA_ERR_UNSUPPORTED 2 /* valid input outside what the kernels implement    */
+#define HEA_ERR_CUDA 3        /* the CUDA runtime reported an error                */
+#define HEA_ERR_NOMEM 4       /* a device or host allocation failed                */
+
+#define HEA_FLAG_LOG_ITERS 1    /* print the per-iteration best fitness line, as accelerate.cu:1208-1212 does */
+#define HEA_FLAG_TIME_KERNELS 2 /* time every local-search launch with CUDA events (hea_stats.mc_ms)        */
+
+/* One structure to search.  Mirrors the arguments nbor, element, weight and
+ * target_sro of run_local_parallel_hcs_cuda (bind.cpp:55-58). */
+typedef struct hea_problem {
+    int32_t num_sites;           /* N = sum of species (accelerate.cu:1128)          */
+    int32_t num_types;           /* T = len(element), 2..6                            */
+    int32_t num_shells;          /* S = len(weight), 1..3 (accelerate.cu:1126)        */
+    const int32_t *shell_sizes;  /* [S] neighbours per site in each shell             */
+    const int32_t *nbor;         /* [N][sum shell_sizes] neighbour ids                */
+    const int32_t *species;      /* [T] atoms of each species ("element")             */
+    const double *weight;        /* [S] shell weights                                 */
+    const double *target_sro;    /* [S][T*T] target Warren-Cowley alpha, row-major    */
+} hea_problem;
+
+/* Search controls: nnet, step, task, depth, thr of the reference call
+ * (bind.cpp:50-54), plus the seed the reference does not take. */
+typedef struct hea_params {
+    int32_t num_solutions;  /* nnet: population size P                               */
+    int32_t total_iter;     /* step: global iterations I                             */
+    int32_t parallel_task;  /* task: proposals scored per round Q                    */
+    int32_t converge_depth; /* depth: rounds without improvement that end a search   */
+    double threshold;       /* thr: accepted and unused, as in the reference         */
+    uint64_t seed;          /* Philox key of every random draw of the search         */
+    int64_t max_rounds;     /* cap on rounds per local search (<= 0: 2^31)           */
+    int32_t flags;          /* HEA_FLAG_*                                            */
+} hea_params;
+
+typedef struct hea_stats {
+    int64_t rounds;   /* search rounds over all local searches                      */
+    int64_t evals;    /* swap evaluations (proposals scored)                        */
+    int64_t accepts;  /* accepted swaps                                             */
+    double gpu_ms;    /* device time of the search, CUDA events                     */
+    double mc_ms;     /* summed device time of the local-search launches (HEA_FLAG_TIME_KERNELS) */
+    int64_t mc_launches; /* local-search launches timed                             */
+} hea_stats;
+
+typedef struct hea_accept_record {
+    uint32_t round, task, s1, s2;
+    double f2;
+} hea_accept_record;
+
+/* accelerate::gpu::cuda_available (accelerate.cu:33-37): 1 if a CUDA device is usable. */
+int hea_cuda_available(void);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char *hea_last_error(void);
+
+/*
+ * The whole search, host buffers in and out: replaces
+ * accelerate::gpu::run_local_parallel_hcs_cuda (accelerate.cu:1112-1242).
+ * out_occ [P][N] receives species ids, out_fitness [P] the fitness
+ * sqrt(f2), both ascending by fitness (the order the reference returns,
+ * pyhea/model/opt.py:103-114 writes entry 0).  stats may be NULL.
+ */
+int hea_run_local_parallel_hcs(const hea_problem *problem, const hea_params *params, uint8_t *out_occ,
+                               double *out_fitness, hea_stats *stats);
+
+/*
+ * Device-resident form of the same search for repeated runs: create uploads
+ * the tables once; run executes the search on the plan's stream and waits for
+ * it; read copies the result out.  Same results as hea_run_local_parallel_hcs
+ * for the same seed.  There is no counterpart call in the reference; it splits
+ * hea_run_local_parallel_hcs at its host/device boundary.
+ */
+typedef struct hea_plan hea_plan;
+int hea_plan_create(const hea_problem *problem, const hea_params *params, hea_plan **out);
+int hea_plan_run(hea_plan *plan, uint64_t seed, hea_stats *stats);
+int hea_plan_read(hea_plan *plan, uint8_t *out_occ, double *out_fitness);
+void hea_plan_destroy(hea_plan *plan);
+
+/*
+ * Component entry points (host buffers), one launch each, used to check the
+ * pieces of the search against the CPU restatement.
+ *
+ * hea_generate: `count` random occupancies of generation `generation`
+ *   (accelerate.cpp:218-252 / accelerate.cu:912-935), with their pair counts
+ *   [count][S][T][T] and f2 [count].
+ * hea_recount: pair counts and f2 of given occupancies (accelerate.cpp:370-399,
+ *   :118-180).
+ * hea_local_search: the local parallel search on `count` occupancies in place
+ *   (accelerate.cpp:601-694 / accelerate.cu:626-731) as local search number
+ *   mc_call of a run; optional trace of accepted swaps (trace_cap records and
+ *   count snapshots per occupancy, trace_len [count]).
+ */
+int hea_generate(const hea_problem *problem, uint64_t seed, uint32_t generation, int32_t count, uint8_t *out_occ,
+                 int32_t *out_counts, double *out_f2);
+int hea_recount(const hea_problem *problem, int32_t count, const uint8_t *occ, int32_t *out_counts, double *out_f2);
+int hea_local_search(const hea_problem *problem, uint64_t seed, uint32_t mc_call, int32_t count, int32_t tasks,
+                     int32_t depth, int64_t max_rounds, uint8_t *occ, int32_t *out_counts, double *out_f2,
+                     int64_t *out_rounds, hea_accept_record *trace, int32_t *trace_counts, int64_t trace_cap,
+                     int64_t *trace_len);
+
+/*
+ * Neighbour table of a perfect cubic supercell built on the device, in the
+ * site numbering and shell order of pyhea/lattice/lattice.py:146-323
+ * (ids sorted within each shell).  lattice: 0 = FCC, 1 = BCC.  shell_set:
+ * 0 = the reference's shells (FCC 12/6/12 with the third shell at sqrt(2) a,
+ * lattice.py:283-287; BCC 8/6/12), 1 = FCC 12/6/24 with the third shell at
+ * sqrt(3/2) a (BCC unchanged).  out_nbor [N][sum sizes] with N = 4 cell^3
+ * (FCC) or 2 cell^3 (BCC); out_shell_sizes [3].  Pass out_nbor = NULL to
+ * query the sizes only.
+ */
+int hea_build_neighbors(int32_t lattice, int32_t cell, int32_t shell_set, int32_t *out_nbor,
+                        int32_t *out_shell_sizes, int32_t *out_num_sites);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HEA_CUDA_H */

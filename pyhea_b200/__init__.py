@@ -1,0 +1,247 @@
+"""B200-native SRO-targeted atom-swap search (the hot path of PyHEA).
+
+Two front ends over one CUDA library (libhea_cuda.so, C ABI in include/hea_cuda.h):
+
+* ``pyhea_b200.accelerate`` -- pybind11 module with the interface of
+  ``pyhea.cpp.accelerate`` (pyhea/cpp/bind.cpp): ``run_local_parallel_hcs_cuda``
+  and ``cuda_available``.  Drop it in as ``pyhea/cpp/accelerate*.so``.
+* the ctypes functions below -- numpy-friendly calls of the same C ABI
+  (``search``, ``Plan``, ``generate``, ``recount``, ``local_search``,
+  ``build_neighbors``), used by the tests and the benchmark.
+
+Importing the package loads the CUDA library and raises ImportError when it has
+not been built (``python -m pyhea_b200.build``); there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_PKG, "libhea_cuda.so")
+if not os.path.exists(_LIB_PATH):
+    raise ImportError(f"{_LIB_PATH} is missing; build it with `python -m pyhea_b200.build`")
+
+_P = ctypes.POINTER
+_i32, _i64, _u32, _u64, _f64, _u8 = (ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32, ctypes.c_uint64,
+                                     ctypes.c_double, ctypes.c_uint8)
+
+HEA_OK, HEA_ERR_INVALID, HEA_ERR_UNSUPPORTED, HEA_ERR_CUDA, HEA_ERR_NOMEM = 0, 1, 2, 3, 4
+HEA_FLAG_LOG_ITERS = 1
+HEA_FLAG_TIME_KERNELS = 2
+FCC, BCC = 0, 1
+SHELLS_REFERENCE, SHELLS_FCC_TRUE3 = 0, 1
+
+
+class HeaError(RuntimeError):
+    """A failed C ABI call; ``code`` is the HEA_ERR_* value."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class HeaValueError(HeaError, ValueError):
+    pass
+
+
+class _Problem(ctypes.Structure):
+    _fields_ = [("num_sites", _i32), ("num_types", _i32), ("num_shells", _i32), ("shell_sizes", _P(_i32)),
+                ("nbor", _P(_i32)), ("species", _P(_i32)), ("weight", _P(_f64)), ("target_sro", _P(_f64))]
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("num_solutions", _i32), ("total_iter", _i32), ("parallel_task", _i32), ("converge_depth", _i32),
+                ("threshold", _f64), ("seed", _u64), ("max_rounds", _i64), ("flags", _i32)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("rounds", _i64), ("evals", _i64), ("accepts", _i64), ("gpu_ms", _f64), ("mc_ms", _f64),
+                ("mc_launches", _i64)]
+
+    def as_dict(self):
+        return {"rounds": self.rounds, "evals": self.evals, "accepts": self.accepts, "gpu_ms": self.gpu_ms,
+                "mc_ms": self.mc_ms, "mc_launches": self.mc_launches}
+
+
+class AcceptRecord(ctypes.Structure):
+    _fields_ = [("round", _u32), ("task", _u32), ("s1", _u32), ("s2", _u32), ("f2", _f64)]
+
+
+def _declare(lib):
+    sig = {
+        "hea_cuda_available": (_i32, []),
+        "hea_last_error": (ctypes.c_char_p, []),
+        "hea_run_local_parallel_hcs": (_i32, [_P(_Problem), _P(_Params), _P(_u8), _P(_f64), _P(Stats)]),
+        "hea_plan_create": (_i32, [_P(_Problem), _P(_Params), _P(ctypes.c_void_p)]),
+        "hea_plan_run": (_i32, [ctypes.c_void_p, _u64, _P(Stats)]),
+        "hea_plan_read": (_i32, [ctypes.c_void_p, _P(_u8), _P(_f64)]),
+        "hea_plan_destroy": (None, [ctypes.c_void_p]),
+        "hea_generate": (_i32, [_P(_Problem), _u64, _u32, _i32, _P(_u8), _P(_i32), _P(_f64)]),
+        "hea_recount": (_i32, [_P(_Problem), _i32, _P(_u8), _P(_i32), _P(_f64)]),
+        "hea_local_search": (_i32, [_P(_Problem), _u64, _u32, _i32, _i32, _i32, _i64, _P(_u8), _P(_i32), _P(_f64),
+                                    _P(_i64), _P(AcceptRecord), _P(_i32), _i64, _P(_i64)]),
+        "hea_build_neighbors": (_i32, [_i32, _i32, _i32, _P(_i32), _P(_i32), _P(_i32)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _declare(ctypes.CDLL(_LIB_PATH))
+from . import accelerate  # noqa: E402  (pybind11 module next to the library)
+
+
+def _check(rc):
+    if rc != HEA_OK:
+        msg = lib.hea_last_error().decode()
+        raise (HeaValueError if rc == HEA_ERR_INVALID else HeaError)(rc, msg)
+
+
+def cuda_available():
+    return bool(lib.hea_cuda_available())
+
+
+def _ptr(a, ct):
+    return a.ctypes.data_as(_P(ct)) if a is not None else None
+
+
+class Problem:
+    """One structure: flattened neighbour table [N][sum Z], shell sizes, species
+    counts, shell weights and target alpha [S][T*T] (the reference's nbor,
+    element, weight and target_sro with nbor cut to len(weight) shells)."""
+
+    def __init__(self, nbor, shell_sizes, species, weight, target_sro):
+        self.species = np.ascontiguousarray(species, dtype=np.int32)
+        self.weight = np.ascontiguousarray(weight, dtype=np.float64)
+        S, T = len(self.weight), len(self.species)
+        sizes = np.asarray(shell_sizes, dtype=np.int32)
+        self.shell_sizes = np.ascontiguousarray(sizes[:S])
+        nb = np.asarray(nbor)
+        self.nbor = np.ascontiguousarray(nb[:, : int(self.shell_sizes.sum())], dtype=np.int32)
+        self.target_sro = np.ascontiguousarray(np.asarray(target_sro, dtype=np.float64).reshape(-1, T * T)[:S])
+        self.num_sites = int(self.species.sum())
+        self.num_types, self.num_shells = T, S
+        self._c = _Problem(self.num_sites, T, S, _ptr(self.shell_sizes, _i32), _ptr(self.nbor, _i32),
+                           _ptr(self.species, _i32), _ptr(self.weight, _f64), _ptr(self.target_sro, _f64))
+
+    @property
+    def ncount(self):
+        return self.num_shells * self.num_types * self.num_types
+
+
+def _params(num_solutions, total_iter, parallel_task, converge_depth, seed, max_rounds=0, flags=0, threshold=0.001):
+    return _Params(int(num_solutions), int(total_iter), int(parallel_task), int(converge_depth), float(threshold),
+                   int(seed) & 0xFFFFFFFFFFFFFFFF, int(max_rounds), int(flags))
+
+
+def search(problem, num_solutions, total_iter, parallel_task, converge_depth, seed=0, max_rounds=0, log=False,
+           out_occ=None, out_fitness=None, time_kernels=False):
+    """The whole search with host buffers (hea_run_local_parallel_hcs).
+    Returns (occ [P][N] uint8, fitness [P] float64, stats dict)."""
+    P, N = int(num_solutions), problem.num_sites
+    occ = out_occ if out_occ is not None else np.empty((P, N), dtype=np.uint8)
+    fit = out_fitness if out_fitness is not None else np.empty(P, dtype=np.float64)
+    st = Stats()
+    flags = (HEA_FLAG_LOG_ITERS if log else 0) | (HEA_FLAG_TIME_KERNELS if time_kernels else 0)
+    prm = _params(P, total_iter, parallel_task, converge_depth, seed, max_rounds, flags)
+    _check(lib.hea_run_local_parallel_hcs(ctypes.byref(problem._c), ctypes.byref(prm), _ptr(occ, _u8),
+                                          _ptr(fit, _f64), ctypes.byref(st)))
+    return occ, fit, st.as_dict()
+
+
+class Plan:
+    """Device-resident search (hea_plan_*): tables uploaded once, run many times."""
+
+    def __init__(self, problem, num_solutions, total_iter, parallel_task, converge_depth, seed=0, max_rounds=0,
+                 time_kernels=False):
+        self.problem = problem
+        self.P = int(num_solutions)
+        self._h = ctypes.c_void_p()
+        prm = _params(num_solutions, total_iter, parallel_task, converge_depth, seed, max_rounds,
+                      HEA_FLAG_TIME_KERNELS if time_kernels else 0)
+        _check(lib.hea_plan_create(ctypes.byref(problem._c), ctypes.byref(prm), ctypes.byref(self._h)))
+
+    def run(self, seed):
+        st = Stats()
+        _check(lib.hea_plan_run(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, ctypes.byref(st)))
+        return st.as_dict()
+
+    def read(self):
+        occ = np.empty((self.P, self.problem.num_sites), dtype=np.uint8)
+        fit = np.empty(self.P, dtype=np.float64)
+        _check(lib.hea_plan_read(self._h, _ptr(occ, _u8), _ptr(fit, _f64)))
+        return occ, fit
+
+    def close(self):
+        if self._h:
+            lib.hea_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def generate(problem, seed, generation, count):
+    """hea_generate: (occ [count][N], counts [count][S][T][T], f2 [count])."""
+    occ = np.empty((count, problem.num_sites), dtype=np.uint8)
+    cnt = np.empty((count, problem.num_shells, problem.num_types, problem.num_types), dtype=np.int32)
+    f2 = np.empty(count)
+    _check(lib.hea_generate(ctypes.byref(problem._c), int(seed), int(generation), int(count), _ptr(occ, _u8),
+                            _ptr(cnt, _i32), _ptr(f2, _f64)))
+    return occ, cnt, f2
+
+
+def recount(problem, occ):
+    """hea_recount: (counts [count][S][T][T], f2 [count]) of occupancies [count][N]."""
+    occ = np.ascontiguousarray(np.atleast_2d(occ), dtype=np.uint8)
+    count = occ.shape[0]
+    cnt = np.empty((count, problem.num_shells, problem.num_types, problem.num_types), dtype=np.int32)
+    f2 = np.empty(count)
+    _check(lib.hea_recount(ctypes.byref(problem._c), int(count), _ptr(occ, _u8), _ptr(cnt, _i32), _ptr(f2, _f64)))
+    return cnt, f2
+
+
+def local_search(problem, seed, mc_call, occ, tasks, depth, max_rounds=0, trace_cap=0, trace_counts=False):
+    """hea_local_search on occupancies [count][N] (copied).  Returns a dict with
+    occ, counts, f2, rounds and, when trace_cap > 0, per-occupancy traces."""
+    occ = np.array(np.atleast_2d(occ), dtype=np.uint8, copy=True)
+    count = occ.shape[0]
+    cnt = np.empty((count, problem.num_shells, problem.num_types, problem.num_types), dtype=np.int32)
+    f2 = np.empty(count)
+    rounds = np.empty(count, dtype=np.int64)
+    tr = (AcceptRecord * max(1, count * trace_cap))() if trace_cap else None
+    tc = (np.empty((count, trace_cap, problem.num_shells, problem.num_types, problem.num_types), dtype=np.int32)
+          if trace_cap and trace_counts else None)
+    tlen = np.zeros(count, dtype=np.int64) if trace_cap else None
+    _check(lib.hea_local_search(ctypes.byref(problem._c), int(seed), int(mc_call), int(count), int(tasks), int(depth),
+                                int(max_rounds), _ptr(occ, _u8), _ptr(cnt, _i32), _ptr(f2, _f64), _ptr(rounds, _i64),
+                                tr, _ptr(tc, _i32), int(trace_cap), _ptr(tlen, _i64)))
+    out = {"occ": occ, "counts": cnt, "f2": f2, "rounds": rounds}
+    if trace_cap:
+        traces = []
+        for p in range(count):
+            n = int(min(tlen[p], trace_cap))
+            recs = [tr[p * trace_cap + i] for i in range(n)]
+            traces.append([(r.round, r.task, r.s1, r.s2, r.f2) for r in recs])
+        out["trace"] = traces
+        out["trace_len"] = tlen
+        out["trace_counts"] = tc
+    return out
+
+
+def build_neighbors(lattice, cell, shell_set=SHELLS_REFERENCE):
+    """Device-built neighbour table of an FCC (0) / BCC (1) cube of edge `cell`:
+    (nbor int32 [N][sum Z], shell_sizes int32 [3])."""
+    sizes = np.zeros(3, dtype=np.int32)
+    n = _i32()
+    _check(lib.hea_build_neighbors(int(lattice), int(cell), int(shell_set), None, _ptr(sizes, _i32), ctypes.byref(n)))
+    nbor = np.empty((n.value, int(sizes.sum())), dtype=np.int32)
+    _check(lib.hea_build_neighbors(int(lattice), int(cell), int(shell_set), _ptr(nbor, _i32), _ptr(sizes, _i32),
+                                   ctypes.byref(n)))
+    return nbor, sizes

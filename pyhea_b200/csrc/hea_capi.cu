@@ -1,0 +1,844 @@
+// hea_capi.cu -- C ABI of the swap-search engine: validation, device tables,
+// the search driver and the component entry points.  Declarations and the
+// reference interfaces they replace: include/hea_cuda.h.
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "hea_cuda.h"
+#include "hea_search.cuh"
+
+using namespace hea;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+    return code;
+}
+
+#define HEA_CUDA(call)                                                                                    \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess) return fail(HEA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define HEA_TRY(expr)            \
+    do {                         \
+        int rc_ = (expr);        \
+        if (rc_ != HEA_OK) return rc_; \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Kernel dispatch over (T, S)
+// ---------------------------------------------------------------------------
+using GenFn = void (*)(const SearchConst, const GenArgs);
+using McFn = void (*)(const SearchConst, const McArgs);
+
+template <int T, int S>
+struct Inst {
+    static constexpr GenFn gen = generate_kernel<T, S>;
+    static constexpr McFn mc = mc_kernel<T, S>;
+};
+
+#define HEA_ROW(T) {nullptr, Inst<T, 1>::gen, Inst<T, 2>::gen, Inst<T, 3>::gen}
+#define HEA_MROW(T) {nullptr, Inst<T, 1>::mc, Inst<T, 2>::mc, Inst<T, 3>::mc}
+const GenFn kGen[kMaxTypes + 1][kMaxShells + 1] = {
+    {nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}, HEA_ROW(2), HEA_ROW(3), HEA_ROW(4),
+    HEA_ROW(5), HEA_ROW(6)};
+const McFn kMc[kMaxTypes + 1][kMaxShells + 1] = {
+    {nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}, HEA_MROW(2), HEA_MROW(3), HEA_MROW(4),
+    HEA_MROW(5), HEA_MROW(6)};
+
+// ---------------------------------------------------------------------------
+// Table preparation kernels
+// ---------------------------------------------------------------------------
+struct PadGeom {
+    int32_t size[kMaxShells], off[kMaxShells], poff[kMaxShells], psize[kMaxShells];
+    int32_t num_shells, raw_row, pad_row, num_sites;
+};
+
+// Padded copy of the raw table plus its checks: id range, no site listed as its
+// own neighbour, and symmetry with multiplicity per shell (the reference's
+// incremental update at accelerate.cpp:526-530 counts each pair from both
+// ends, which equals a recount only on such tables).  err bits: 1 range,
+// 2 self, 4 asymmetric.
+__global__ void pad_and_check_kernel(const int32_t *raw, int32_t *padded, PadGeom g, int *err)
+{
+    const int64_t total = (int64_t)g.num_sites * g.pad_row;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
+        const int s = (int)(x / g.pad_row), e = (int)(x % g.pad_row);
+        int k = 0;
+        while (k + 1 < g.num_shells && e >= g.poff[k + 1]) ++k;
+        const int q = e - g.poff[k];
+        if (q >= g.size[k]) {
+            padded[x] = g.num_sites;
+            continue;
+        }
+        const int n = raw[(int64_t)s * g.raw_row + g.off[k] + q];
+        padded[x] = n;
+        if (n < 0 || n >= g.num_sites) {
+            atomicOr(err, 1);
+            continue;
+        }
+        if (n == s) {
+            atomicOr(err, 2);
+            continue;
+        }
+        // multiplicity of n in s's shell k must equal that of s in n's shell k
+        const int32_t *rs = raw + (int64_t)s * g.raw_row + g.off[k];
+        const int32_t *rn = raw + (int64_t)n * g.raw_row + g.off[k];
+        int fwd = 0, back = 0;
+        for (int j = 0; j < g.size[k]; ++j) {
+            fwd += rs[j] == n;
+            back += rn[j] == s;
+        }
+        if (fwd != back) atomicOr(err, 4);
+    }
+}
+
+__global__ void gather_rows_kernel(const uint8_t *occ, const int32_t *order, int count, int stride, int n,
+                                   const double *f2, uint8_t *out, double *out_f2)
+{
+    const int p = blockIdx.y;
+    if (p >= count) return;
+    const uint8_t *src = occ + (size_t)order[p] * stride;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) out[(size_t)p * n + s] = src[s];
+    if (blockIdx.x == 0 && threadIdx.x == 0) out_f2[p] = f2[order[p]];
+}
+
+__global__ void scatter_rows_kernel(const uint8_t *in, int count, int stride, int n, uint8_t *occ)
+{
+    const int p = blockIdx.y;
+    if (p >= count) return;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x)
+        occ[(size_t)p * stride + s] = in[(size_t)p * n + s];
+}
+
+__global__ void iota_kernel(int32_t *order, int count)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) order[i] = i;
+}
+
+// ---------------------------------------------------------------------------
+// Lattice neighbour tables (pyhea/lattice/lattice.py:146-323)
+// Positions in half lattice units; site id = nb * (x L^2 + y L + z) + basis.
+// ---------------------------------------------------------------------------
+struct LatticeSpec {
+    int nb;                // basis sites per cell
+    int basis[4][3];       // basis offsets, half units
+    int nshell, size[3];   // shells
+    int vec[3][24][3];     // offsets per shell, half units
+};
+
+__device__ __forceinline__ int basis_of(const LatticeSpec &sp, int px, int py, int pz)
+{
+    for (int b = 0; b < sp.nb; ++b)
+        if ((sp.basis[b][0] & 1) == (px & 1) && (sp.basis[b][1] & 1) == (py & 1) && (sp.basis[b][2] & 1) == (pz & 1))
+            return b;
+    return -1;
+}
+
+__global__ void build_neighbors_kernel(LatticeSpec sp, int L, int32_t *out, int row, int *err)
+{
+    const int n = sp.nb * L * L * L;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const int b = s % sp.nb, cell = s / sp.nb;
+        const int cx = cell / (L * L), cy = (cell / L) % L, cz = cell % L;
+        const int px = 2 * cx + sp.basis[b][0], py = 2 * cy + sp.basis[b][1], pz = 2 * cz + sp.basis[b][2];
+        int32_t *o = out + (size_t)s * row;
+        for (int k = 0; k < sp.nshell; ++k) {
+            int ids[24];
+            for (int v = 0; v < sp.size[k]; ++v) {
+                const int qx = ((px + sp.vec[k][v][0]) % (2 * L) + 2 * L) % (2 * L);
+                const int qy = ((py + sp.vec[k][v][1]) % (2 * L) + 2 * L) % (2 * L);
+                const int qz = ((pz + sp.vec[k][v][2]) % (2 * L) + 2 * L) % (2 * L);
+                const int nb = basis_of(sp, qx, qy, qz);
+                if (nb < 0) {
+                    atomicOr(err, 1);
+                    ids[v] = 0;
+                    continue;
+                }
+                ids[v] = sp.nb * ((qx >> 1) * L * L + (qy >> 1) * L + (qz >> 1)) + nb;
+            }
+            for (int i = 1; i < sp.size[k]; ++i) {  // ascending, as np.sort
+                const int x = ids[i];
+                int j = i - 1;
+                while (j >= 0 && ids[j] > x) {
+                    ids[j + 1] = ids[j];
+                    --j;
+                }
+                ids[j + 1] = x;
+            }
+            for (int v = 0; v < sp.size[k]; ++v) o[v] = ids[v];
+            o += sp.size[k];
+        }
+    }
+}
+
+int make_lattice_spec(int lattice, int shell_set, LatticeSpec &sp)
+{
+    std::memset(&sp, 0, sizeof(sp));
+    auto add_perms = [&](int k, int a, int b, int c) {
+        // all sign/axis placements of (a, b, c) with |a|,|b|,|c| given, unique
+        std::vector<std::array<int, 3>> got;
+        const int base[3] = {a, b, c};
+        const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+        for (auto &p : perm)
+            for (int sx = -1; sx <= 1; sx += 2)
+                for (int sy = -1; sy <= 1; sy += 2)
+                    for (int sz = -1; sz <= 1; sz += 2) {
+                        std::array<int, 3> v = {sx * base[p[0]], sy * base[p[1]], sz * base[p[2]]};
+                        bool dup = false;
+                        for (auto &u : got) dup = dup || (u == v);
+                        if (!dup) got.push_back(v);
+                    }
+        sp.size[k] = (int)got.size();
+        for (size_t i = 0; i < got.size(); ++i)
+            for (int d = 0; d < 3; ++d) sp.vec[k][i][d] = got[i][d];
+    };
+    sp.nshell = 3;
+    if (lattice == 0) {  // FCC, lattice.py:168-194,261-323
+        sp.nb = 4;
+        const int bs[4][3] = {{0, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}};
+        std::memcpy(sp.basis, bs, sizeof(bs));
+        add_perms(0, 1, 1, 0);
+        add_perms(1, 2, 0, 0);
+        if (shell_set == 0)
+            add_perms(2, 2, 2, 0);
+        else
+            add_perms(2, 2, 1, 1);
+    } else if (lattice == 1) {  // BCC, lattice.py:146-166,196-259
+        sp.nb = 2;
+        const int bs[2][3] = {{0, 0, 0}, {1, 1, 1}};
+        std::memcpy(sp.basis, bs, sizeof(bs));
+        add_perms(0, 1, 1, 1);
+        add_perms(1, 2, 0, 0);
+        add_perms(2, 2, 2, 0);
+    } else {
+        return fail(HEA_ERR_INVALID, "lattice must be 0 (FCC) or 1 (BCC), got %d", lattice);
+    }
+    return HEA_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Validated problem with its device tables
+// ---------------------------------------------------------------------------
+struct DeviceTables {
+    SearchConst c{};
+    int T = 0, S = 0, N = 0;
+    int64_t ncount = 0;
+    int4 *nbor = nullptr;
+    size_t smem_gen = 0, smem_mc = 0;
+    GenFn gen = nullptr;
+    McFn mc = nullptr;
+    int mc_block = 0;
+    ~DeviceTables()
+    {
+        if (nbor) cudaFree(nbor);
+    }
+};
+
+int validate_problem(const hea_problem *pb)
+{
+    if (!pb) return fail(HEA_ERR_INVALID, "problem is NULL");
+    if (pb->num_types < 1) return fail(HEA_ERR_INVALID, "element must name at least one species");
+    if (pb->num_types < 2 || pb->num_types > kMaxTypes)
+        return fail(HEA_ERR_UNSUPPORTED, "number of species must be 2..%d, got %d", kMaxTypes, pb->num_types);
+    if (pb->num_shells < 1 || pb->num_shells > kMaxShells)
+        return fail(HEA_ERR_UNSUPPORTED, "number of shells (len(weight)) must be 1..%d, got %d", kMaxShells,
+                    pb->num_shells);
+    if (!pb->shell_sizes || !pb->nbor || !pb->species || !pb->weight || !pb->target_sro)
+        return fail(HEA_ERR_INVALID, "problem has a NULL array");
+    int64_t n = 0;
+    for (int t = 0; t < pb->num_types; ++t) {
+        if (pb->species[t] < 1)
+            return fail(HEA_ERR_INVALID, "species %d has %d atoms; every species needs at least one", t, pb->species[t]);
+        n += pb->species[t];
+    }
+    if (n != pb->num_sites)
+        return fail(HEA_ERR_INVALID, "num_sites %d differs from the sum of element counts %lld", pb->num_sites,
+                    (long long)n);
+    if (n < 2 || n > (int64_t)INT32_MAX / 2) return fail(HEA_ERR_INVALID, "number of sites %lld out of range", (long long)n);
+    for (int k = 0; k < pb->num_shells; ++k) {
+        if (pb->shell_sizes[k] < 1) return fail(HEA_ERR_INVALID, "shell %d is empty", k);
+        if (((pb->shell_sizes[k] + 3) & ~3) > kMaxShellPad)
+            return fail(HEA_ERR_UNSUPPORTED, "shell %d has %d neighbours; at most %d are supported", k,
+                        pb->shell_sizes[k], kMaxShellPad);
+        if (!std::isfinite(pb->weight[k]) || pb->weight[k] < 0)
+            return fail(HEA_ERR_INVALID, "weight[%d] = %g must be finite and >= 0", k, pb->weight[k]);
+        for (int x = 0; x < pb->num_types * pb->num_types; ++x)
+            if (!std::isfinite(pb->target_sro[(size_t)k * pb->num_types * pb->num_types + x]))
+                return fail(HEA_ERR_INVALID, "target_sro[%d][%d] is not finite", k, x);
+    }
+    return HEA_OK;
+}
+
+int validate_params(const hea_params *pr)
+{
+    if (!pr) return fail(HEA_ERR_INVALID, "params is NULL");
+    if (pr->num_solutions < 1 || pr->num_solutions > 65535)
+        return fail(HEA_ERR_INVALID, "nnet must be 1..65535, got %d", pr->num_solutions);
+    if (pr->total_iter < 0 || pr->total_iter > 32766)
+        return fail(HEA_ERR_INVALID, "step must be 0..32766, got %d", pr->total_iter);
+    if (pr->parallel_task < 1) return fail(HEA_ERR_INVALID, "task must be >= 1, got %d", pr->parallel_task);
+    if (pr->converge_depth < 0) return fail(HEA_ERR_INVALID, "depth must be >= 0, got %d", pr->converge_depth);
+    return HEA_OK;
+}
+
+int smem_limit()
+{
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return v;
+}
+
+int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt)
+{
+    HEA_TRY(validate_problem(pb));
+    const int T = pb->num_types, S = pb->num_shells, N = pb->num_sites;
+    dt.T = T;
+    dt.S = S;
+    dt.N = N;
+    dt.ncount = (int64_t)S * T * T;
+    SearchConst &c = dt.c;
+    std::memset(&c, 0, sizeof(c));
+    PadGeom g{};
+    int raw_row = 0;
+    for (int k = 0; k < S; ++k) raw_row += pb->shell_sizes[k];
+    int off = 0, poff = 0;
+    for (int k = 0; k < S; ++k) {
+        const int z = pb->shell_sizes[k], zp = (z + 3) & ~3;
+        g.size[k] = z;
+        g.off[k] = off;
+        g.poff[k] = poff;
+        g.psize[k] = zp;
+        c.off4[k] = poff / 4;
+        c.chunks[k] = zp / 4;
+        c.pad[k] = zp - z;
+        off += z;
+        poff += zp;
+    }
+    g.num_shells = S;
+    g.raw_row = raw_row;
+    g.pad_row = poff;
+    g.num_sites = N;
+    c.row4 = poff / 4;
+    c.num_sites = N;
+    c.num_types = T;
+    c.num_shells = S;
+    c.occ_stride = (N + 15) & ~15;
+    c.feistel_h = feistel_half_bits((uint32_t)N);
+    c.reject_below = (uint32_t)(0u - (uint32_t)N) % (uint32_t)N;
+    c.key0 = (uint32_t)seed;
+    c.key1 = (uint32_t)(seed >> 32);
+    c.prefix[0] = 0;
+    for (int t = 0; t < T; ++t) c.prefix[t + 1] = c.prefix[t] + pb->species[t];
+    for (int k = 0; k < S; ++k) {
+        c.w[k] = pb->weight[k];
+        for (int i = 0; i < T; ++i)
+            for (int j = 0; j < T; ++j) {
+                const int e = (k * T + i) * T + j;
+                c.E[e] = 1.0 - pb->target_sro[(size_t)k * T * T + i * T + j];
+                c.R[e] = (double)N / (((double)pb->shell_sizes[k] * (double)pb->species[i]) * (double)pb->species[j]);
+            }
+    }
+
+    // shared memory of the two kernels
+    const size_t cnt_bytes = 4 * (size_t)((dt.ncount + 3) & ~3);
+    dt.smem_gen = (size_t)c.occ_stride + 16 + cnt_bytes;
+    dt.smem_mc = (size_t)c.occ_stride + 16 + cnt_bytes + 32 * 8 + 32 * 4 + 16;
+    if (dt.smem_mc > (size_t)smem_limit())
+        return fail(HEA_ERR_UNSUPPORTED,
+                    "%d sites need %zu bytes of shared memory per solution, above the %d-byte limit of the "
+                    "shared-memory search path",
+                    N, dt.smem_mc, smem_limit());
+    dt.gen = kGen[T][S];
+    dt.mc = kMc[T][S];
+    HEA_CUDA(cudaFuncSetAttribute(dt.gen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dt.smem_gen));
+    HEA_CUDA(cudaFuncSetAttribute(dt.mc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dt.smem_mc));
+
+    // padded table on the device, checked
+    const size_t raw_bytes = (size_t)N * raw_row * sizeof(int32_t);
+    const size_t pad_bytes = (size_t)N * poff * sizeof(int32_t);
+    int32_t *raw = nullptr;
+    int *derr = nullptr;
+    HEA_CUDA(cudaMalloc(&raw, raw_bytes));
+    if (cudaMalloc(&dt.nbor, pad_bytes) != cudaSuccess || cudaMalloc(&derr, sizeof(int)) != cudaSuccess) {
+        cudaFree(raw);
+        return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes for the neighbour table", pad_bytes);
+    }
+    int herr = 0;
+    cudaError_t e = cudaMemcpy(raw, pb->nbor, raw_bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(derr, 0, sizeof(int));
+    if (e == cudaSuccess) {
+        pad_and_check_kernel<<<1184, 256>>>(raw, reinterpret_cast<int32_t *>(dt.nbor), g, derr);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(raw);
+    cudaFree(derr);
+    if (e != cudaSuccess) return fail(HEA_ERR_CUDA, "neighbour table upload failed: %s", cudaGetErrorString(e));
+    if (herr & 1) return fail(HEA_ERR_INVALID, "neighbour list holds an id outside [0, %d)", N);
+    if (herr & 2) return fail(HEA_ERR_UNSUPPORTED, "neighbour list names a site as its own neighbour");
+    if (herr & 4)
+        return fail(HEA_ERR_UNSUPPORTED,
+                    "neighbour list is not symmetric within a shell (site a lists b a different number of times "
+                    "than b lists a)");
+    return HEA_OK;
+}
+
+int choose_block(int tasks)
+{
+    int b = ((tasks + 31) / 32) * 32;
+    if (b > 512) b = 512;
+    return b;
+}
+
+struct DeviceBuf {
+    void *p = nullptr;
+    ~DeviceBuf()
+    {
+        if (p) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Plan
+// ---------------------------------------------------------------------------
+struct hea_plan {
+    DeviceTables dt;
+    hea_params prm{};
+    int P = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint8_t *occ = nullptr, *out_occ = nullptr;
+    int32_t *cnt = nullptr, *order = nullptr, *scratch = nullptr;
+    double *f2 = nullptr, *out_f2 = nullptr;
+    unsigned long long *stats = nullptr;
+    std::vector<cudaEvent_t> mc_events;  // start/stop pairs, HEA_FLAG_TIME_KERNELS
+    int mc_timed = 0;
+    ~hea_plan()
+    {
+        for (cudaEvent_t e : mc_events) cudaEventDestroy(e);
+        for (void *p : {(void *)occ, (void *)out_occ, (void *)cnt, (void *)order, (void *)scratch, (void *)f2,
+                        (void *)out_f2, (void *)stats})
+            if (p) cudaFree(p);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+int launch_generate(hea_plan *pl, const int32_t *order, int count, uint32_t generation, int generate)
+{
+    GenArgs a{};
+    a.nbor = pl->dt.nbor;
+    a.occ = pl->occ;
+    a.cnt = pl->cnt;
+    a.f2 = pl->f2;
+    a.order = order;
+    a.generation = generation;
+    a.generate = generate;
+    pl->dt.gen<<<count, 512, pl->dt.smem_gen, pl->stream>>>(pl->dt.c, a);
+    HEA_CUDA(cudaGetLastError());
+    return HEA_OK;
+}
+
+int launch_mc(hea_plan *pl, const int32_t *order, int count, uint32_t mc_call, McArgs extra)
+{
+    McArgs a = extra;
+    a.nbor = pl->dt.nbor;
+    a.occ = pl->occ;
+    a.cnt = pl->cnt;
+    a.f2 = pl->f2;
+    a.order = order;
+    a.mc_call = mc_call;
+    a.tasks = pl->prm.parallel_task;
+    a.depth = pl->prm.converge_depth;
+    a.max_rounds = pl->prm.max_rounds > 0 ? pl->prm.max_rounds : (int64_t)1 << 31;
+    a.stats = pl->stats;
+    const bool timed = (pl->prm.flags & HEA_FLAG_TIME_KERNELS) && 2 * pl->mc_timed + 1 < (int)pl->mc_events.size();
+    if (timed) HEA_CUDA(cudaEventRecord(pl->mc_events[2 * pl->mc_timed], pl->stream));
+    pl->dt.mc<<<count, choose_block(a.tasks), pl->dt.smem_mc, pl->stream>>>(pl->dt.c, a);
+    HEA_CUDA(cudaGetLastError());
+    if (timed) {
+        HEA_CUDA(cudaEventRecord(pl->mc_events[2 * pl->mc_timed + 1], pl->stream));
+        ++pl->mc_timed;
+    }
+    return HEA_OK;
+}
+
+int launch_sort(hea_plan *pl, int32_t *order, int count)
+{
+    sort_slots_kernel<<<1, 1024, 0, pl->stream>>>(order, pl->f2, count, pl->scratch);
+    HEA_CUDA(cudaGetLastError());
+    return HEA_OK;
+}
+
+int plan_alloc(hea_plan *pl, int slots)
+{
+    const SearchConst &c = pl->dt.c;
+    HEA_CUDA(cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking));
+    HEA_CUDA(cudaEventCreate(&pl->ev0));
+    HEA_CUDA(cudaEventCreate(&pl->ev1));
+    const size_t occ_bytes = (size_t)slots * c.occ_stride;
+    if (cudaMalloc(&pl->occ, occ_bytes) != cudaSuccess ||
+        cudaMalloc(&pl->cnt, (size_t)slots * pl->dt.ncount * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&pl->order, (size_t)slots * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&pl->scratch, (size_t)slots * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&pl->f2, (size_t)slots * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&pl->out_occ, (size_t)slots * c.num_sites) != cudaSuccess ||
+        cudaMalloc(&pl->out_f2, (size_t)slots * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&pl->stats, 4 * sizeof(unsigned long long)) != cudaSuccess)
+        return fail(HEA_ERR_NOMEM, "cannot allocate the population buffers (%zu bytes of occupancy)", occ_bytes);
+    HEA_CUDA(cudaMemsetAsync(pl->occ, 0, occ_bytes, pl->stream));
+    iota_kernel<<<(slots + 255) / 256, 256, 0, pl->stream>>>(pl->order, slots);
+    HEA_CUDA(cudaGetLastError());
+    return HEA_OK;
+}
+
+void log_iteration(int it, double best)
+{
+    std::time_t now = std::time(nullptr);
+    char ts[32];
+    std::strftime(ts, sizeof(ts), "%Y-%m-%d %H:%M:%S", std::localtime(&now));
+    std::printf("%s - PyHEA - INFO - Iter %d with best fitness:      %g\n", ts, it, best);
+    std::fflush(stdout);
+}
+
+int read_population(hea_plan *pl, int count, uint8_t *out_occ, double *out_fitness)
+{
+    const SearchConst &c = pl->dt.c;
+    dim3 grid((c.num_sites + 255) / 256 < 64 ? (c.num_sites + 255) / 256 : 64, count);
+    gather_rows_kernel<<<grid, 256, 0, pl->stream>>>(pl->occ, pl->order, count, c.occ_stride, c.num_sites, pl->f2,
+                                                     pl->out_occ, pl->out_f2);
+    HEA_CUDA(cudaGetLastError());
+    if (out_occ)
+        HEA_CUDA(cudaMemcpyAsync(out_occ, pl->out_occ, (size_t)count * c.num_sites, cudaMemcpyDeviceToHost, pl->stream));
+    std::vector<double> f(count);
+    HEA_CUDA(cudaMemcpyAsync(f.data(), pl->out_f2, count * sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
+    HEA_CUDA(cudaStreamSynchronize(pl->stream));
+    if (out_fitness)
+        for (int p = 0; p < count; ++p) out_fitness[p] = std::sqrt(f[p]);
+    return HEA_OK;
+}
+
+// The global loop of accelerate.cpp:737-761: generation 0, then per iteration a
+// new population searched (call 2*it), merged (stable, current first), and the
+// survivors searched (call 2*it+1) and sorted.
+int plan_search(hea_plan *pl, hea_stats *stats)
+{
+    const int P = pl->P;
+    pl->mc_timed = 0;
+    if ((pl->prm.flags & HEA_FLAG_TIME_KERNELS) && pl->mc_events.size() < (size_t)(4 * pl->prm.total_iter)) {
+        while (pl->mc_events.size() < (size_t)(4 * pl->prm.total_iter)) {
+            cudaEvent_t e;
+            HEA_CUDA(cudaEventCreate(&e));
+            pl->mc_events.push_back(e);
+        }
+    }
+    HEA_CUDA(cudaMemsetAsync(pl->stats, 0, 4 * sizeof(unsigned long long), pl->stream));
+    iota_kernel<<<(2 * P + 255) / 256, 256, 0, pl->stream>>>(pl->order, 2 * P);
+    HEA_CUDA(cudaGetLastError());
+    HEA_CUDA(cudaEventRecord(pl->ev0, pl->stream));
+    HEA_TRY(launch_generate(pl, pl->order, P, 0, 1));
+    for (int it = 0; it < pl->prm.total_iter; ++it) {
+        HEA_TRY(launch_generate(pl, pl->order + P, P, (uint32_t)(it + 1), 1));
+        HEA_TRY(launch_mc(pl, pl->order + P, P, (uint32_t)(2 * it), McArgs{}));
+        HEA_TRY(launch_sort(pl, pl->order, 2 * P));
+        HEA_TRY(launch_mc(pl, pl->order, P, (uint32_t)(2 * it + 1), McArgs{}));
+        HEA_TRY(launch_sort(pl, pl->order, P));
+        if (pl->prm.flags & HEA_FLAG_LOG_ITERS) {
+            int32_t best_slot = 0;
+            double best = 0;
+            HEA_CUDA(cudaMemcpyAsync(&best_slot, pl->order, sizeof(int32_t), cudaMemcpyDeviceToHost, pl->stream));
+            HEA_CUDA(cudaStreamSynchronize(pl->stream));
+            HEA_CUDA(cudaMemcpyAsync(&best, pl->f2 + best_slot, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
+            HEA_CUDA(cudaStreamSynchronize(pl->stream));
+            log_iteration(it, std::sqrt(best));
+        }
+    }
+    HEA_CUDA(cudaEventRecord(pl->ev1, pl->stream));
+    HEA_CUDA(cudaStreamSynchronize(pl->stream));
+    if (stats) {
+        unsigned long long s[4];
+        HEA_CUDA(cudaMemcpy(s, pl->stats, sizeof(s), cudaMemcpyDeviceToHost));
+        float ms = 0;
+        HEA_CUDA(cudaEventElapsedTime(&ms, pl->ev0, pl->ev1));
+        stats->rounds = (int64_t)s[0];
+        stats->evals = (int64_t)s[1];
+        stats->accepts = (int64_t)s[2];
+        stats->gpu_ms = ms;
+        stats->mc_ms = 0;
+        stats->mc_launches = pl->mc_timed;
+        for (int i = 0; i < pl->mc_timed; ++i) {
+            float m = 0;
+            HEA_CUDA(cudaEventElapsedTime(&m, pl->mc_events[2 * i], pl->mc_events[2 * i + 1]));
+            stats->mc_ms += m;
+        }
+    }
+    return HEA_OK;
+}
+
+int plan_create(const hea_problem *pb, const hea_params *prm, int slots, hea_plan **out)
+{
+    *out = nullptr;
+    hea_plan *pl = new (std::nothrow) hea_plan();
+    if (!pl) return fail(HEA_ERR_NOMEM, "out of host memory");
+    int rc = build_tables(pb, prm->seed, pl->dt);
+    if (rc == HEA_OK) {
+        pl->prm = *prm;
+        pl->P = prm->num_solutions;
+        rc = plan_alloc(pl, slots);
+    }
+    if (rc != HEA_OK) {
+        delete pl;
+        return rc;
+    }
+    *out = pl;
+    return HEA_OK;
+}
+
+hea_params component_params(int count, int tasks, int depth, int64_t max_rounds, uint64_t seed)
+{
+    hea_params p{};
+    p.num_solutions = count;
+    p.total_iter = 0;
+    p.parallel_task = tasks;
+    p.converge_depth = depth;
+    p.seed = seed;
+    p.max_rounds = max_rounds;
+    return p;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Public entry points
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int hea_cuda_available(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n > 0;
+}
+
+const char *hea_last_error(void) { return g_error.c_str(); }
+
+int hea_plan_create(const hea_problem *problem, const hea_params *params, hea_plan **out)
+{
+    if (!out) return fail(HEA_ERR_INVALID, "out is NULL");
+    HEA_TRY(validate_params(params));
+    return plan_create(problem, params, 2 * params->num_solutions, out);
+}
+
+int hea_plan_run(hea_plan *plan, uint64_t seed, hea_stats *stats)
+{
+    if (!plan) return fail(HEA_ERR_INVALID, "plan is NULL");
+    plan->dt.c.key0 = (uint32_t)seed;
+    plan->dt.c.key1 = (uint32_t)(seed >> 32);
+    plan->prm.seed = seed;
+    return plan_search(plan, stats);
+}
+
+int hea_plan_read(hea_plan *plan, uint8_t *out_occ, double *out_fitness)
+{
+    if (!plan) return fail(HEA_ERR_INVALID, "plan is NULL");
+    return read_population(plan, plan->P, out_occ, out_fitness);
+}
+
+void hea_plan_destroy(hea_plan *plan) { delete plan; }
+
+int hea_run_local_parallel_hcs(const hea_problem *problem, const hea_params *params, uint8_t *out_occ,
+                               double *out_fitness, hea_stats *stats)
+{
+    hea_plan *pl = nullptr;
+    HEA_TRY(hea_plan_create(problem, params, &pl));
+    int rc = plan_search(pl, stats);
+    if (rc == HEA_OK) rc = read_population(pl, pl->P, out_occ, out_fitness);
+    delete pl;
+    return rc;
+}
+
+int hea_generate(const hea_problem *problem, uint64_t seed, uint32_t generation, int32_t count, uint8_t *out_occ,
+                 int32_t *out_counts, double *out_f2)
+{
+    if (count < 1 || count > 65535) return fail(HEA_ERR_INVALID, "count must be 1..65535");
+    hea_params p = component_params(count, 1, 0, 0, seed);
+    hea_plan *pl = nullptr;
+    HEA_TRY(plan_create(problem, &p, count, &pl));
+    int rc = launch_generate(pl, pl->order, count, generation, 1);
+    if (rc == HEA_OK && out_counts) {
+        cudaError_t e = cudaMemcpyAsync(out_counts, pl->cnt, (size_t)count * pl->dt.ncount * sizeof(int32_t),
+                                        cudaMemcpyDeviceToHost, pl->stream);
+        if (e != cudaSuccess) rc = fail(HEA_ERR_CUDA, "copy of counts failed: %s", cudaGetErrorString(e));
+    }
+    if (rc == HEA_OK) rc = read_population(pl, count, out_occ, nullptr);
+    if (rc == HEA_OK && out_f2) {
+        cudaError_t e = cudaMemcpy(out_f2, pl->f2, count * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail(HEA_ERR_CUDA, "copy of f2 failed: %s", cudaGetErrorString(e));
+    }
+    delete pl;
+    return rc;
+}
+
+namespace {
+int load_occupancy(hea_plan *pl, int count, const uint8_t *occ)
+{
+    const SearchConst &c = pl->dt.c;
+    const int T = pl->dt.T;
+    for (size_t x = 0; x < (size_t)count * c.num_sites; ++x)
+        if (occ[x] >= T) return fail(HEA_ERR_INVALID, "occupancy holds species %d >= %d", occ[x], T);
+    for (int p = 0; p < count; ++p) {  // composition must match element
+        std::vector<int64_t> h(T, 0);
+        for (int s = 0; s < c.num_sites; ++s) ++h[occ[(size_t)p * c.num_sites + s]];
+        for (int t = 0; t < T; ++t)
+            if (h[t] != c.prefix[t + 1] - c.prefix[t])
+                return fail(HEA_ERR_INVALID, "occupancy %d has %lld atoms of species %d, element says %d", p,
+                            (long long)h[t], t, c.prefix[t + 1] - c.prefix[t]);
+    }
+    HEA_CUDA(cudaMemcpyAsync(pl->out_occ, occ, (size_t)count * c.num_sites, cudaMemcpyHostToDevice, pl->stream));
+    dim3 grid((c.num_sites + 255) / 256 < 64 ? (c.num_sites + 255) / 256 : 64, count);
+    scatter_rows_kernel<<<grid, 256, 0, pl->stream>>>(pl->out_occ, count, c.occ_stride, c.num_sites, pl->occ);
+    HEA_CUDA(cudaGetLastError());
+    return launch_generate(pl, pl->order, count, 0, 0);
+}
+}  // namespace
+
+int hea_recount(const hea_problem *problem, int32_t count, const uint8_t *occ, int32_t *out_counts, double *out_f2)
+{
+    if (count < 1 || count > 65535) return fail(HEA_ERR_INVALID, "count must be 1..65535");
+    if (!occ) return fail(HEA_ERR_INVALID, "occ is NULL");
+    hea_params p = component_params(count, 1, 0, 0, 0);
+    hea_plan *pl = nullptr;
+    HEA_TRY(plan_create(problem, &p, count, &pl));
+    int rc = load_occupancy(pl, count, occ);
+    if (rc == HEA_OK && out_counts) {
+        cudaError_t e = cudaMemcpyAsync(out_counts, pl->cnt, (size_t)count * pl->dt.ncount * sizeof(int32_t),
+                                        cudaMemcpyDeviceToHost, pl->stream);
+        if (e != cudaSuccess) rc = fail(HEA_ERR_CUDA, "copy of counts failed: %s", cudaGetErrorString(e));
+    }
+    if (rc == HEA_OK) rc = read_population(pl, count, nullptr, nullptr);
+    if (rc == HEA_OK && out_f2) {
+        cudaError_t e = cudaMemcpy(out_f2, pl->f2, count * sizeof(double), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail(HEA_ERR_CUDA, "copy of f2 failed: %s", cudaGetErrorString(e));
+    }
+    delete pl;
+    return rc;
+}
+
+int hea_local_search(const hea_problem *problem, uint64_t seed, uint32_t mc_call, int32_t count, int32_t tasks,
+                     int32_t depth, int64_t max_rounds, uint8_t *occ, int32_t *out_counts, double *out_f2,
+                     int64_t *out_rounds, hea_accept_record *trace, int32_t *trace_counts, int64_t trace_cap,
+                     int64_t *trace_len)
+{
+    if (count < 1 || count > 65535) return fail(HEA_ERR_INVALID, "count must be 1..65535");
+    if (tasks < 1) return fail(HEA_ERR_INVALID, "tasks must be >= 1");
+    if (depth < 0) return fail(HEA_ERR_INVALID, "depth must be >= 0");
+    if (mc_call > 65534) return fail(HEA_ERR_INVALID, "mc_call must be <= 65534");
+    if (!occ) return fail(HEA_ERR_INVALID, "occ is NULL");
+    if (trace_cap < 0 || (trace_cap > 0 && (!trace || !trace_len)))
+        return fail(HEA_ERR_INVALID, "trace needs trace, trace_len and trace_cap >= 0");
+    hea_params p = component_params(count, tasks, depth, max_rounds, seed);
+    hea_plan *pl = nullptr;
+    HEA_TRY(plan_create(problem, &p, count, &pl));
+    int rc = load_occupancy(pl, count, occ);
+    DeviceBuf dtrace, dtc, dlen, drounds;
+    const size_t ncount = (size_t)pl->dt.ncount;
+    McArgs extra{};
+    if (rc == HEA_OK) {
+        if (cudaMalloc(&drounds.p, count * sizeof(int64_t)) != cudaSuccess) rc = fail(HEA_ERR_NOMEM, "no memory");
+        extra.rounds_out = (int64_t *)drounds.p;
+        if (rc == HEA_OK && trace_cap > 0) {
+            if (cudaMalloc(&dtrace.p, (size_t)count * trace_cap * sizeof(AcceptRecord)) != cudaSuccess ||
+                cudaMalloc(&dlen.p, count * sizeof(int64_t)) != cudaSuccess ||
+                (trace_counts &&
+                 cudaMalloc(&dtc.p, (size_t)count * trace_cap * ncount * sizeof(int32_t)) != cudaSuccess))
+                rc = fail(HEA_ERR_NOMEM, "cannot allocate the trace buffers");
+            extra.trace = (AcceptRecord *)dtrace.p;
+            extra.trace_counts = (int32_t *)dtc.p;
+            extra.trace_len = (int64_t *)dlen.p;
+            extra.trace_cap = trace_cap;
+        }
+    }
+    if (rc == HEA_OK) {
+        cudaMemsetAsync(pl->stats, 0, 4 * sizeof(unsigned long long), pl->stream);
+        rc = launch_mc(pl, pl->order, count, mc_call, extra);
+    }
+    if (rc == HEA_OK) rc = read_population(pl, count, occ, nullptr);
+    auto copy = [&](void *dst, const void *src, size_t bytes) {
+        if (rc != HEA_OK || !dst || !src) return;
+        cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = fail(HEA_ERR_CUDA, "copy failed: %s", cudaGetErrorString(e));
+    };
+    copy(out_counts, pl->cnt, (size_t)count * ncount * sizeof(int32_t));
+    copy(out_f2, pl->f2, count * sizeof(double));
+    copy(out_rounds, drounds.p, count * sizeof(int64_t));
+    if (trace_cap > 0) {
+        copy(trace, dtrace.p, (size_t)count * trace_cap * sizeof(AcceptRecord));
+        copy(trace_len, dlen.p, count * sizeof(int64_t));
+        copy(trace_counts, dtc.p, (size_t)count * trace_cap * ncount * sizeof(int32_t));
+    }
+    delete pl;
+    return rc;
+}
+
+int hea_build_neighbors(int32_t lattice, int32_t cell, int32_t shell_set, int32_t *out_nbor, int32_t *out_shell_sizes,
+                        int32_t *out_num_sites)
+{
+    if (cell < 1 || cell > 1024) return fail(HEA_ERR_INVALID, "cell must be 1..1024, got %d", cell);
+    if (shell_set != 0 && shell_set != 1) return fail(HEA_ERR_INVALID, "shell_set must be 0 or 1");
+    LatticeSpec sp;
+    HEA_TRY(make_lattice_spec(lattice, shell_set, sp));
+    const int64_t n = (int64_t)sp.nb * cell * cell * cell;
+    if (n > INT32_MAX / 2) return fail(HEA_ERR_INVALID, "cell %d gives too many sites", cell);
+    int row = 0;
+    for (int k = 0; k < 3; ++k) {
+        row += sp.size[k];
+        if (out_shell_sizes) out_shell_sizes[k] = sp.size[k];
+    }
+    if (out_num_sites) *out_num_sites = (int32_t)n;
+    if (!out_nbor) return HEA_OK;
+    DeviceBuf d, derr;
+    const size_t bytes = (size_t)n * row * sizeof(int32_t);
+    if (cudaMalloc(&d.p, bytes) != cudaSuccess || cudaMalloc(&derr.p, sizeof(int)) != cudaSuccess)
+        return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes for the neighbour table", bytes);
+    HEA_CUDA(cudaMemset(derr.p, 0, sizeof(int)));
+    const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+    build_neighbors_kernel<<<blocks, 256>>>(sp, cell, (int32_t *)d.p, row, (int *)derr.p);
+    HEA_CUDA(cudaGetLastError());
+    int herr = 0;
+    HEA_CUDA(cudaMemcpy(&herr, derr.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) return fail(HEA_ERR_INVALID, "lattice construction produced an off-lattice position");
+    HEA_CUDA(cudaMemcpy(out_nbor, d.p, bytes, cudaMemcpyDeviceToHost));
+    return HEA_OK;
+}
+
+}  // extern "C"

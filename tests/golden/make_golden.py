@@ -1,0 +1,162 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Run in a checkout that has the reference tree (default /root/reference, or
+HEA_REFERENCE_ROOT) and the reference CPU engine built by
+oracle/build_oracle.py:
+
+    python oracle/build_oracle.py && python tests/golden/make_golden.py
+
+Fixtures written:
+  nbor_ref.npz       neighbour lists produced by the reference lattice builder
+                     (pyhea/lattice/lattice.py:196-323) for FCC/BCC cells of edge 3 and 4
+  target_sro.json    lower-triangle TARGET_SRO files expanded by the reference
+                     config reader (pyhea/io/input.py:350-465) for 2-4 species
+  ref_engine.npz     per-case occupancies and swaps with the reference engine's
+                     gamma (accelerate.cpp:370-399), full fitness (:118-180) and
+                     incremental fitness (:498-570)
+
+The reference's Python modules import mpi4py, OVITO, dpdata and matplotlib at
+module level; none is needed by the two functions used here, so they are
+replaced by stubs in sys.modules before the import.
+"""
+import ctypes
+import json
+import os
+import sys
+import tempfile
+from unittest import mock
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REFERENCE_ROOT = os.environ.get("HEA_REFERENCE_ROOT", "/root/reference")
+
+
+def import_reference():
+    for name in ["mpi4py", "ovito", "ovito.io", "ovito.modifiers", "ovito.data", "WarrenCowleyParameters", "dpdata",
+                 "matplotlib", "matplotlib.pyplot", "psutil"]:
+        sys.modules.setdefault(name, mock.MagicMock())
+    sys.path.insert(0, REFERENCE_ROOT)
+    from pyhea.lattice.lattice import lattice  # noqa: E402
+    from pyhea.io.input import input_config  # noqa: E402
+    return lattice, input_config
+
+
+def flat_nbor(nbor):
+    return np.array([np.concatenate([np.asarray(sh, dtype=np.int64) for sh in site]) for site in nbor], dtype=np.int32)
+
+
+def main():
+    lattice, input_config = import_reference()
+
+    # 1. neighbour lists
+    nb = {}
+    for typ in ("FCC", "BCC"):
+        for L in (3, 4):
+            lat = lattice([L, L, L], typ, 1.0, np.eye(3) * L)
+            nb[f"{typ}_{L}"] = flat_nbor(lat.nbor_list)
+            nb[f"{typ}_{L}_shells"] = np.array([len(s) for s in lat.nbor_list[0]], dtype=np.int32)
+    np.savez_compressed(os.path.join(HERE, "nbor_ref.npz"), **nb)
+
+    # 2. TARGET_SRO expansion (lower triangle per shell -> full T*T matrices)
+    cases = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for T in (2, 3, 4):
+            m = T * (T + 1) // 2
+            shells = [[round(0.01 * (k + 1) * (q + 1) - 0.05, 4) for q in range(m)] for k in range(3)]
+            lines = []
+            for k, vals in enumerate(shells):
+                lines.append(["First Shell", "Second Shell", "Third Shell"][k])
+                pos = 0
+                for row in range(T):
+                    lines.append(" ".join(str(v) for v in vals[pos:pos + row + 1]))
+                    pos += row + 1
+            path = os.path.join(tmp, f"TARGET_SRO_{T}")
+            with open(path, "w") as f:
+                f.write("\n".join(lines) + "\n")
+            cfg = object.__new__(input_config)
+            cfg.config = {"type": T, "target_sro": path}
+            cwd = os.getcwd()
+            os.chdir("/")
+            try:
+                full = np.asarray(cfg.target_sro, dtype=float)
+            finally:
+                os.chdir(cwd)
+            cases[str(T)] = {"lower": shells, "full": full.tolist()}
+        cfg = object.__new__(input_config)
+        cfg.config = {"type": 4}
+        cases["default_4"] = {"lower": None, "full": np.asarray(cfg.target_sro, dtype=float).tolist()}
+    with open(os.path.join(HERE, "target_sro.json"), "w") as f:
+        json.dump(cases, f, indent=1)
+
+    # 3. reference engine functions on fixed occupancies and swaps
+    ref = ctypes.CDLL(os.path.join(REPO, "oracle", "_ref", "libref_accelerate.so"))
+    ref.ref_fitness_incremental.restype = ctypes.c_double
+    P = ctypes.POINTER
+    i32 = lambda a: a.ctypes.data_as(P(ctypes.c_int32))  # noqa: E731
+    f64 = lambda a: a.ctypes.data_as(P(ctypes.c_double))  # noqa: E731
+    rng = np.random.default_rng(20241203)
+    specs = [
+        ("fcc4_t4_s3", "FCC_4", [64, 64, 64, 64], [4.0, 1.0, 0.5]),
+        ("bcc4_t3_s2", "BCC_4", [40, 44, 44], [1.0, 0.5]),
+        ("fcc3_t5_s3", "FCC_3", [20, 22, 22, 22, 22], [4.0, 1.0, 0.5]),
+        ("bcc4_t6_s3", "BCC_4", [20, 20, 20, 20, 24, 24], [2.0, 1.0, 0.25]),
+        ("fcc4_t2_s1", "FCC_4", [100, 156], [1.0]),
+    ]
+    out = {}
+    for name, key, species, weight in specs:
+        nbor_full = nb[key]
+        shells_full = nb[key + "_shells"]
+        S = len(weight)
+        T = len(species)
+        N = int(sum(species))
+        assert N == nbor_full.shape[0]
+        shell_size = shells_full[:S].copy()
+        nbor = np.ascontiguousarray(nbor_full[:, : int(shell_size.sum())])
+        row = nbor.shape[1]
+        tgt = rng.uniform(-0.2, 0.2, size=(S, T, T))
+        tgt = 0.5 * (tgt + tgt.transpose(0, 2, 1))
+        target = np.ascontiguousarray(tgt.reshape(S, T * T))
+        sp = np.array(species, dtype=np.int32)
+        w = np.array(weight, dtype=np.float64)
+        layout = np.repeat(np.arange(T, dtype=np.int32), species)
+        occs = np.stack([rng.permutation(layout) for _ in range(4)]).astype(np.int32)
+        gam = np.zeros((4, T, T, S))
+        for p in range(4):
+            ref.ref_recount(N, T, S, i32(nbor), row, i32(shell_size), i32(sp), i32(np.ascontiguousarray(occs[p])),
+                            f64(gam[p]))
+        fit = np.zeros(4)
+        ref.ref_fitness_of_solutions(4, N, T, S, i32(nbor), row, i32(shell_size), i32(sp), f64(w), f64(target),
+                                     i32(occs), f64(fit))
+        # swaps on occupancy 0: half random pairs, half first-shell neighbour pairs
+        swaps, inc_fit, inc_gam = [], [], []
+        occ0 = np.ascontiguousarray(occs[0])
+        while len(swaps) < 24:
+            a = int(rng.integers(N))
+            b = int(rng.integers(N)) if len(swaps) % 2 == 0 else int(nbor[a, rng.integers(shell_size[0])])
+            if occ0[a] == occ0[b]:
+                continue
+            g_out = np.zeros((T, T, S))
+            f = ref.ref_fitness_incremental(N, T, S, i32(nbor), row, i32(shell_size), i32(sp), f64(w), f64(target),
+                                            i32(occ0), a, b, f64(np.ascontiguousarray(gam[0])), f64(g_out))
+            swaps.append((a, b))
+            inc_fit.append(f)
+            inc_gam.append(g_out)
+        out[name + "/lattice"] = np.array(key)
+        out[name + "/species"] = sp
+        out[name + "/weight"] = w
+        out[name + "/target"] = target
+        out[name + "/shell_size"] = shell_size
+        out[name + "/occ"] = occs
+        out[name + "/gamma"] = gam
+        out[name + "/fitness"] = fit
+        out[name + "/swaps"] = np.array(swaps, dtype=np.int32)
+        out[name + "/swap_fitness"] = np.array(inc_fit)
+        out[name + "/swap_gamma"] = np.array(inc_gam)
+    np.savez_compressed(os.path.join(HERE, "ref_engine.npz"), **out)
+    print("wrote", sorted(os.listdir(HERE)))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,210 @@
+"""CUDA path vs the CPU oracle, through the C ABI (and the pybind11 drop-in).
+
+Integer results (occupancies, pair counts, accepted-swap traces) must be
+bit-exact; f2 is computed with the same fused multiply-adds in the same order
+on both sides, so it must be bit-exact too.  Fitness against the reference
+engine's own floating-point accumulation: 1e-12 relative.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from conftest import REPO, engine_case_problem
+from oracle import hea_oracle as ho
+import pyhea_b200 as hb
+from pyhea_b200 import lattice as L
+from pyhea_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    # lattice, cell, species, shells, shell_set
+    (L.FCC, 4, (64, 64, 64, 64), 3, L.SHELLS_REFERENCE),
+    (L.BCC, 5, (40, 42, 42, 42, 42, 42), 3, L.SHELLS_REFERENCE),
+    (L.FCC, 3, (20, 22, 22, 22, 22), 3, L.SHELLS_FCC_TRUE3),
+    (L.BCC, 4, (40, 44, 44), 2, L.SHELLS_REFERENCE),
+    (L.FCC, 4, (100, 156), 1, L.SHELLS_REFERENCE),
+    (L.BCC, 3, (1, 53), 3, L.SHELLS_REFERENCE),  # 54 sites (not a multiple of 16), one minority atom
+]
+
+
+def pair(case, seed=0):
+    lat, cell, species, shells, shell_set = case
+    st = W.small_case(lattice=lat, cell=cell, species=species, shells=shells, shell_set=shell_set, seed=seed)
+    nbor, sizes = st.neighbors()
+    return (hb.Problem(nbor, sizes, st.species, st.weight, st.target),
+            ho.Problem(nbor[:, : int(sizes[:shells].sum())], sizes[:shells], st.species, st.weight, st.target))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_generate_bit_exact(case):
+    gp, op = pair(case)
+    occ, cnt, f2 = hb.generate(gp, seed=1234, generation=3, count=5)
+    for s in range(5):
+        want = op.generate(1234, 3, s)
+        np.testing.assert_array_equal(occ[s], want)
+        C = op.recount(want)
+        np.testing.assert_array_equal(cnt[s], C)
+        assert f2[s] == op.f2(C)
+
+
+def test_recount_matches_reference_engine(golden_engine, golden_nbor):
+    for name, case in golden_engine.items():
+        gp = engine_case_problem(case, golden_nbor, hb)
+        op = engine_case_problem(case, golden_nbor, ho)
+        cnt, f2 = hb.recount(gp, case["occ"].astype(np.uint8))
+        ss = case["shell_size"]
+        for p in range(len(case["occ"])):
+            ref = np.rint(case["gamma"][p].transpose(2, 0, 1) * ss[:, None, None] * gp.num_sites).astype(np.int64)
+            np.testing.assert_array_equal(cnt[p], ref, err_msg=name)
+            assert f2[p] == op.f2(ref)
+            assert abs(np.sqrt(f2[p]) - case["fitness"][p]) <= 1e-12 * case["fitness"][p]
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("tasks", [1, 37, 64, 600])
+def test_local_search_trajectory_bit_exact(case, tasks):
+    """Every accepted swap (round, task, sites, f2) and the counts after it equal the oracle's."""
+    gp, op = pair(case)
+    count, depth, call = 3, 4, 7
+    occ0 = np.stack([op.generate(99, 2, s) for s in range(count)])
+    got = hb.local_search(gp, 99, call, occ0, tasks, depth, trace_cap=4096, trace_counts=True)
+    for s in range(count):
+        want = op.mc(99, (call << 16) | s, occ0[s], tasks, depth, trace_cap=4096, trace_counts=True)
+        assert got["rounds"][s] == want["rounds"]
+        assert got["trace_len"][s] == want["accepts"]
+        assert got["trace"][s] == want["trace"]
+        n = len(want["trace"])
+        np.testing.assert_array_equal(got["trace_counts"][s][:n], want["trace_counts"])
+        np.testing.assert_array_equal(got["occ"][s], want["occ"])
+        np.testing.assert_array_equal(got["counts"][s], want["counts"])
+        assert got["f2"][s] == want["f2"]
+        # counts maintained on the device == a recount of the final occupancy
+        np.testing.assert_array_equal(got["counts"][s], op.recount(got["occ"][s]))
+
+
+@pytest.mark.parametrize("case", CASES[:4])
+def test_full_search_bit_exact(case):
+    gp, op = pair(case)
+    occ, fit, stats = hb.search(gp, num_solutions=4, total_iter=2, parallel_task=32, converge_depth=4, seed=77)
+    wocc, wf2, wstats = op.hcs(77, 4, 2, 32, 4)
+    np.testing.assert_array_equal(occ, wocc)
+    np.testing.assert_array_equal(fit, np.sqrt(wf2))
+    assert stats["evals"] == wstats["evals"] and stats["accepts"] == wstats["accepts"]
+    assert stats["rounds"] == wstats["rounds"]
+
+
+def test_plan_reruns_match_search():
+    gp, _ = pair(CASES[0])
+    occ, fit, _ = hb.search(gp, 6, 2, 48, 3, seed=5)
+    plan = hb.Plan(gp, 6, 2, 48, 3)
+    for _ in range(2):
+        plan.run(5)
+        pocc, pfit = plan.read()
+        np.testing.assert_array_equal(pocc, occ)
+        np.testing.assert_array_equal(pfit, fit)
+    plan.run(6)
+    assert not np.array_equal(plan.read()[0], occ)
+    plan.close()
+
+
+def test_dropin_module_call_as_pyhea_model_makes_it():
+    """The positional call of pyhea/model/opt.py:89-90 with nested neighbour lists."""
+    lat, cell, species = L.FCC, 4, [64, 64, 64, 64]
+    nbor, sizes = L.neighbors(lat, cell)
+    nested = L.as_nested(nbor, sizes)
+    st = W.small_case(lattice=lat, cell=cell, species=species)
+    target = st.target  # ndarray [3][T*T], as input_config.target_sro returns
+    assert hb.accelerate.cuda_available() is True
+    latts, fitss = hb.accelerate.run_local_parallel_hcs_cuda(4, 2, 32, 4, 0.001, nested, species, [4.0, 1.0, 0.5],
+                                                             target, seed=77, verbose=False)
+    assert isinstance(latts, list) and isinstance(latts[0], list) and isinstance(latts[0][0], int)
+    assert isinstance(fitss, list) and fitss == sorted(fitss)
+    op = ho.Problem(nbor, sizes, species, [4.0, 1.0, 0.5], target)
+    wocc, wf2, _ = op.hcs(77, 4, 2, 32, 4)
+    np.testing.assert_array_equal(np.array(latts), wocc)
+    np.testing.assert_array_equal(np.array(fitss), np.sqrt(wf2))
+
+
+def test_search_fitness_agrees_with_reference_engine():
+    """Final structures scored by the reference's calculate_fitness_of_solutions."""
+    path = os.path.join(REPO, "oracle", "_ref", "libref_accelerate.so")
+    if not os.path.exists(path):
+        pytest.skip("reference engine not built")
+    ref = ctypes.CDLL(path)
+    gp, op = pair(CASES[1])
+    occ, fit, _ = hb.search(gp, 4, 2, 64, 4, seed=3)
+    rf = np.zeros(4)
+    P = ctypes.POINTER
+    occ32 = occ.astype(np.int32)
+    ref.ref_fitness_of_solutions(4, gp.num_sites, gp.num_types, gp.num_shells, gp.nbor.ctypes.data_as(P(ctypes.c_int32)),
+                                 gp.nbor.shape[1], gp.shell_sizes.ctypes.data_as(P(ctypes.c_int32)),
+                                 gp.species.ctypes.data_as(P(ctypes.c_int32)), gp.weight.ctypes.data_as(P(ctypes.c_double)),
+                                 gp.target_sro.ctypes.data_as(P(ctypes.c_double)), occ32.ctypes.data_as(P(ctypes.c_int32)),
+                                 rf.ctypes.data_as(P(ctypes.c_double)))
+    np.testing.assert_allclose(fit, rf, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("lat", [L.FCC, L.BCC])
+@pytest.mark.parametrize("shell_set", [L.SHELLS_REFERENCE, L.SHELLS_FCC_TRUE3])
+@pytest.mark.parametrize("cell", [2, 3, 5, 7])
+def test_device_neighbor_builder(lat, shell_set, cell):
+    d, ds = hb.build_neighbors(lat, cell, shell_set)
+    h, hs = L.neighbors(lat, cell, shell_set)
+    np.testing.assert_array_equal(ds, hs)
+    np.testing.assert_array_equal(d, h)
+
+
+def test_edge_controls():
+    gp, op = pair(CASES[0])
+    # no iterations: the initial population in generation order
+    occ, fit, st = hb.search(gp, 3, 0, 8, 3, seed=9)
+    for s in range(3):
+        np.testing.assert_array_equal(occ[s], op.generate(9, 0, s))
+    assert st["evals"] == 0
+    # depth 0: no rounds; one solution, one task
+    occ, fit, st = hb.search(gp, 1, 2, 1, 0, seed=9)
+    assert st["rounds"] == 0
+    wocc, wf2, _ = op.hcs(9, 1, 2, 1, 0)
+    np.testing.assert_array_equal(occ, wocc)
+    # round cap
+    r = hb.local_search(gp, 9, 0, op.generate(9, 1, 0)[None], 16, 1000, max_rounds=5)
+    assert r["rounds"][0] == 5
+
+
+def test_bad_tables_are_rejected():
+    nbor, sizes = L.neighbors(L.FCC, 4)
+    T = 4
+    bad = nbor.copy()
+    bad[3, 0] = 10_000
+    with pytest.raises(ValueError, match="outside"):
+        hb.search(hb.Problem(bad, sizes, [64] * T, [4.0, 1.0, 0.5], np.zeros((3, 16))), 2, 1, 8, 2)
+    bad = nbor.copy()
+    bad[3, 0] = bad[3, 1]  # duplicate breaks symmetry with multiplicity
+    with pytest.raises(hb.HeaError, match="symmetric"):
+        hb.search(hb.Problem(bad, sizes, [64] * T, [4.0, 1.0, 0.5], np.zeros((3, 16))), 2, 1, 8, 2)
+    bad = nbor.copy()
+    bad[3, 0] = 3
+    with pytest.raises(hb.HeaError, match="own neighbour"):
+        hb.search(hb.Problem(bad, sizes, [64] * T, [4.0, 1.0, 0.5], np.zeros((3, 16))), 2, 1, 8, 2)
+
+
+def test_full_size_plain_gpu_properties():
+    """The BCC 20^3 five-species structure at full size (fewer iterations):
+    composition kept, output ascending, every fitness equal to a recount's."""
+    st = W.plain_gpu(seed=0)
+    gp = st.problem(device=True)
+    occ, fit, stats = hb.search(gp, st.P, 2, st.Q, st.D, seed=11)
+    assert np.all(np.diff(fit) >= 0)
+    for o in occ[:: max(1, st.P // 16)]:
+        np.testing.assert_array_equal(np.bincount(o, minlength=5), st.species)
+    cnt, f2 = hb.recount(gp, occ)
+    np.testing.assert_array_equal(np.sqrt(f2), fit)
+    op = ho.Problem(gp.nbor, gp.shell_sizes, gp.species, gp.weight, gp.target_sro)
+    for p in (0, st.P - 1):
+        np.testing.assert_array_equal(cnt[p], op.recount(occ[p]))
+    assert stats["evals"] > 0 and stats["accepts"] > 0
+    init = hb.generate(gp, 11, 0, st.P)[2]
+    assert fit[0] ** 2 < init.min()

@@ -1,0 +1,141 @@
+"""The CPU restatement (oracle/) pinned against the reference engine and its
+published primitives; CPU only."""
+import numpy as np
+import pytest
+
+from conftest import engine_case_problem
+from oracle import hea_oracle as ho
+from pyhea_b200 import lattice as L
+from pyhea_b200 import workloads as W
+
+# Random123 known-answer vectors for Philox4x32-10 (kat_vectors of the SC'11 release)
+PHILOX_KAT = [
+    ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+    ((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2, (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+    ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+     (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+]
+
+
+@pytest.mark.parametrize("ctr,key,want", PHILOX_KAT)
+def test_philox_known_answers(ctr, key, want):
+    assert tuple(ho.philox(ctr, key)) == want
+
+
+def test_recount_matches_reference_engine(golden_engine, golden_nbor):
+    """Counts == gamma * Z_k * N of calculate_sro_coefficient (accelerate.cpp:370-399), exactly."""
+    for name, case in golden_engine.items():
+        pr = engine_case_problem(case, golden_nbor, ho)
+        ss = case["shell_size"]
+        for occ, gam in zip(case["occ"], case["gamma"]):
+            C = pr.recount(occ.astype(np.uint8))
+            scaled = gam.transpose(2, 0, 1) * ss[:, None, None] * pr.num_sites
+            ref = np.rint(scaled).astype(np.int64)
+            assert np.abs(scaled - ref).max() < 1e-6, name
+            np.testing.assert_array_equal(C, ref, err_msg=name)
+
+
+def test_fitness_matches_reference_engine(golden_engine, golden_nbor):
+    """sqrt(f2) agrees with calculate_fitness_of_solutions (accelerate.cpp:118-180) to 1e-12 relative."""
+    for name, case in golden_engine.items():
+        pr = engine_case_problem(case, golden_nbor, ho)
+        for occ, fit in zip(case["occ"], case["fitness"]):
+            f = np.sqrt(pr.f2(pr.recount(occ.astype(np.uint8))))
+            assert abs(f - fit) <= 1e-12 * fit, (name, f, fit)
+
+
+def test_incremental_matches_reference_engine(golden_engine, golden_nbor):
+    """Swap update == calculate_fitness_incremental (accelerate.cpp:498-570): counts exact, fitness 1e-12."""
+    for name, case in golden_engine.items():
+        pr = engine_case_problem(case, golden_nbor, ho)
+        ss = case["shell_size"]
+        occ = case["occ"][0].astype(np.uint8)
+        C0 = pr.recount(occ)
+        for (a, b), fit, gam in zip(case["swaps"], case["swap_fitness"], case["swap_gamma"]):
+            Cp = pr.swap_counts(occ, C0, a, b)
+            ref = np.rint(gam.transpose(2, 0, 1) * ss[:, None, None] * pr.num_sites).astype(np.int64)
+            np.testing.assert_array_equal(Cp, ref, err_msg=name)
+            after = occ.copy()
+            after[a], after[b] = after[b], after[a]
+            np.testing.assert_array_equal(Cp, pr.recount(after))
+            assert abs(np.sqrt(pr.f2(Cp)) - fit) <= 1e-12 * fit, name
+
+
+def test_generate_keeps_composition_and_is_a_permutation():
+    st = W.small_case(species=(50, 70, 80, 56))
+    nbor, ss = st.neighbors()
+    pr = ho.Problem(nbor, ss, st.species, st.weight, st.target)
+    for slot in range(3):
+        perm = ho.permutation(7, 1, slot, pr.num_sites)
+        assert sorted(perm.tolist()) == list(range(pr.num_sites))
+        occ = pr.generate(7, 1, slot)
+        np.testing.assert_array_equal(np.bincount(occ, minlength=4), st.species)
+    assert not np.array_equal(pr.generate(7, 1, 0), pr.generate(7, 1, 1))
+    assert not np.array_equal(pr.generate(7, 1, 0), pr.generate(8, 1, 0))
+
+
+def test_generate_is_uniform_per_site():
+    """Species frequency at fixed sites over many keys matches the composition (chi-square)."""
+    st = W.small_case(lattice=L.BCC, cell=3, species=(9, 18, 27))
+    nbor, ss = st.neighbors()
+    pr = ho.Problem(nbor, ss, st.species, st.weight, st.target)
+    hits = np.zeros((pr.num_sites, 3))
+    R = 600
+    for seed in range(R):
+        occ = pr.generate(seed, 0, 0)
+        hits[np.arange(pr.num_sites), occ] += 1
+    expect = R * st.species / st.species.sum()
+    chi2 = (((hits - expect) ** 2) / expect).sum()
+    dof = pr.num_sites * 2
+    assert abs(chi2 - dof) < 6 * np.sqrt(2 * dof), (chi2, dof)
+
+
+def test_draw_pair_uniform_and_valid():
+    st = W.small_case(lattice=L.BCC, cell=3, species=(20, 34))
+    nbor, ss = st.neighbors()
+    pr = ho.Problem(nbor, ss, st.species, st.weight, st.target)
+    occ = pr.generate(1, 0, 0)
+    seen = np.zeros(pr.num_sites)
+    for q in range(4000):
+        att, a, b = pr.draw_pair(3, 5, 0, q, occ)
+        assert att >= 0 and occ[a] != occ[b]
+        seen[a] += 1
+    # s1 is uniform over sites given validity weight: species-0 sites are picked with prob ∝ n1
+    p0 = seen[occ == 0].sum() / seen.sum()
+    assert abs(p0 - 0.5) < 0.05
+
+
+def test_mc_counts_match_recount_after_every_accept():
+    st = W.small_case(species=(64, 64, 64, 64))
+    nbor, ss = st.neighbors()
+    pr = ho.Problem(nbor, ss, st.species, st.weight, st.target)
+    occ0 = pr.generate(11, 1, 0)
+    res = pr.mc(11, 5, occ0, tasks=16, depth=4, trace_cap=5000, trace_counts=True)
+    assert res["accepts"] > 10
+    occ = occ0.copy()
+    last = np.inf
+    for (rnd, task, s1, s2, f2), cnt in zip(res["trace"], res["trace_counts"]):
+        occ[s1], occ[s2] = occ[s2], occ[s1]
+        np.testing.assert_array_equal(cnt, pr.recount(occ))
+        assert f2 == pr.f2(cnt) and f2 < last
+        last = f2
+    np.testing.assert_array_equal(occ, res["occ"])
+    np.testing.assert_array_equal(res["counts"], pr.recount(occ))
+    assert res["evals"] <= res["rounds"] * 16
+
+
+def test_hcs_sorted_deterministic_and_improving():
+    st = W.small_case(species=(64, 64, 64, 64))
+    nbor, ss = st.neighbors()
+    pr = ho.Problem(nbor, ss, st.species, st.weight, st.target)
+    occ, f2, stats = pr.hcs(3, num_solutions=4, total_iter=2, tasks=16, depth=4)
+    assert np.all(np.diff(f2) >= 0)
+    for o, f in zip(occ, f2):
+        np.testing.assert_array_equal(np.bincount(o, minlength=4), st.species)
+        assert pr.f2(pr.recount(o)) == f
+    occ2, f22, _ = pr.hcs(3, num_solutions=4, total_iter=2, tasks=16, depth=4)
+    np.testing.assert_array_equal(occ, occ2)
+    np.testing.assert_array_equal(f2, f22)
+    init = [pr.f2(pr.recount(pr.generate(3, 0, s))) for s in range(4)]
+    assert f2[0] < min(init)
+    assert stats["evals"] > 0 and stats["accepts"] > 0
