@@ -33,7 +33,8 @@
  *              the reference's gamma is C / (Z_k * N).
  *   Fitness    f2 = sum_k w_k * sum_i sum_j d^2 with d = fma(-C', R, E),
  *              E = 1 - target, R = N / (Z_k * n_i * n_j), accumulated with
- *              fma in the order k, i, j.  Fitness reported = sqrt(f2); every
+ *              fma per shell over the upper triangle row by row (d_ii, then
+ *              d_ij, d_ji for j > i).  Fitness reported = sqrt(f2); every
  *              comparison is made on f2.
  *   Ties       lowest task index wins the round (strict <), accept iff strictly
  *              better; populations are sorted stably by f2.
@@ -225,18 +226,32 @@ void hea_oracle_recount(const hea_oracle_problem *p, const uint8_t *occ, int32_t
     }
 }
 
+/*
+ * f2 of a count matrix.  Per shell the squares are accumulated with fma over
+ * the upper triangle row by row: the diagonal term d_ii, then for every j > i
+ * the pair d_ij, d_ji.  f2 = fma(w_k, e_k, f2) over the shells in order.
+ */
+static double term_d(const hea_oracle_problem *p, const int32_t *C, int x)
+{
+    return fma(-(double)C[x], p->R[x], p->E[x]);
+}
+
 double hea_oracle_f2(const hea_oracle_problem *p, const int32_t *C)
 {
     int T = p->num_types;
     double f2 = 0.0;
     for (int k = 0; k < p->num_shells; ++k) {
         double e = 0.0;
-        for (int i = 0; i < T; ++i)
-            for (int j = 0; j < T; ++j) {
-                int x = (k * T + i) * T + j;
-                double d = fma(-(double)C[x], p->R[x], p->E[x]);
-                e = fma(d, d, e);
+        for (int i = 0; i < T; ++i) {
+            double dii = term_d(p, C, (k * T + i) * T + i);
+            e = fma(dii, dii, e);
+            for (int j = i + 1; j < T; ++j) {
+                double dij = term_d(p, C, (k * T + i) * T + j);
+                double dji = term_d(p, C, (k * T + j) * T + i);
+                e = fma(dij, dij, e);
+                e = fma(dji, dji, e);
             }
+        }
         f2 = fma(p->weight[k], e, f2);
     }
     return f2;

@@ -3,6 +3,7 @@
 // reference interfaces they replace: include/hea_cuda.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdarg>
@@ -51,20 +52,39 @@ int fail(int code, const char *fmt, ...)
 using GenFn = void (*)(const SearchConst, const GenArgs);
 using McFn = void (*)(const SearchConst, const McArgs);
 
-template <int T, int S>
-struct Inst {
-    static constexpr GenFn gen = generate_kernel<T, S>;
-    static constexpr McFn mc = mc_kernel<T, S>;
-};
-
-#define HEA_ROW(T) {nullptr, Inst<T, 1>::gen, Inst<T, 2>::gen, Inst<T, 3>::gen}
-#define HEA_MROW(T) {nullptr, Inst<T, 1>::mc, Inst<T, 2>::mc, Inst<T, 3>::mc}
+#define HEA_GEN_ROW(T) {nullptr, generate_kernel<T, 1>, generate_kernel<T, 2>, generate_kernel<T, 3>}
 const GenFn kGen[kMaxTypes + 1][kMaxShells + 1] = {
-    {nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}, HEA_ROW(2), HEA_ROW(3), HEA_ROW(4),
-    HEA_ROW(5), HEA_ROW(6)};
-const McFn kMc[kMaxTypes + 1][kMaxShells + 1] = {
-    {nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}, HEA_MROW(2), HEA_MROW(3), HEA_MROW(4),
-    HEA_MROW(5), HEA_MROW(6)};
+    {nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}, HEA_GEN_ROW(2), HEA_GEN_ROW(3),
+    HEA_GEN_ROW(4), HEA_GEN_ROW(5), HEA_GEN_ROW(6)};
+
+// Local-search kernel for species count T and the table's padded shell layout:
+// the layouts of the FCC/BCC shell sets (in int4 chunks per shell) have their
+// loads unrolled; any other table uses the runtime-layout instance.
+template <int T>
+McFn pick_mc_t(int c0, int c1, int c2, int S)
+{
+    if (c0 == 2 && c1 == 0 && c2 == 0) return mc_kernel<T, Shells<2, 0, 0>>;  // BCC, 1 shell
+    if (c0 == 2 && c1 == 2 && c2 == 0) return mc_kernel<T, Shells<2, 2, 0>>;  // BCC, 2 shells
+    if (c0 == 2 && c1 == 2 && c2 == 3) return mc_kernel<T, Shells<2, 2, 3>>;  // BCC 8/6/12
+    if (c0 == 3 && c1 == 0 && c2 == 0) return mc_kernel<T, Shells<3, 0, 0>>;  // FCC, 1 shell
+    if (c0 == 3 && c1 == 2 && c2 == 0) return mc_kernel<T, Shells<3, 2, 0>>;  // FCC, 2 shells
+    if (c0 == 3 && c1 == 2 && c2 == 3) return mc_kernel<T, Shells<3, 2, 3>>;  // FCC 12/6/12
+    if (c0 == 3 && c1 == 2 && c2 == 6) return mc_kernel<T, Shells<3, 2, 6>>;  // FCC 12/6/24
+    if (S == 1) return mc_kernel<T, RuntimeShells<1>>;
+    if (S == 2) return mc_kernel<T, RuntimeShells<2>>;
+    return mc_kernel<T, RuntimeShells<3>>;
+}
+
+McFn pick_mc(int T, int c0, int c1, int c2, int S)
+{
+    switch (T) {
+    case 2: return pick_mc_t<2>(c0, c1, c2, S);
+    case 3: return pick_mc_t<3>(c0, c1, c2, S);
+    case 4: return pick_mc_t<4>(c0, c1, c2, S);
+    case 5: return pick_mc_t<5>(c0, c1, c2, S);
+    default: return pick_mc_t<6>(c0, c1, c2, S);
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Table preparation kernels
@@ -310,6 +330,18 @@ int smem_limit()
     return v;
 }
 
+size_t mc_smem(int occ_stride, int ncount, int nwarps)
+{
+    return (size_t)occ_stride + 16 + (size_t)nwarps * 4 * mc_ncount_pad(ncount) + 2 * 32 * sizeof(SwapRecord);
+}
+
+int choose_block(int tasks)
+{
+    int b = ((tasks + 31) / 32) * 32;
+    if (b > 512) b = 512;
+    return b;
+}
+
 int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt)
 {
     HEA_TRY(validate_problem(pb));
@@ -364,14 +396,14 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt)
     // shared memory of the two kernels
     const size_t cnt_bytes = 4 * (size_t)((dt.ncount + 3) & ~3);
     dt.smem_gen = (size_t)c.occ_stride + 16 + cnt_bytes;
-    dt.smem_mc = (size_t)c.occ_stride + 16 + cnt_bytes + 32 * 8 + 32 * 4 + 16;
+    dt.smem_mc = mc_smem(c.occ_stride, (int)dt.ncount, 16);  // the largest block (512 threads)
     if (dt.smem_mc > (size_t)smem_limit())
         return fail(HEA_ERR_UNSUPPORTED,
                     "%d sites need %zu bytes of shared memory per solution, above the %d-byte limit of the "
                     "shared-memory search path",
                     N, dt.smem_mc, smem_limit());
     dt.gen = kGen[T][S];
-    dt.mc = kMc[T][S];
+    dt.mc = pick_mc(T, c.chunks[0], S > 1 ? c.chunks[1] : 0, S > 2 ? c.chunks[2] : 0, S);
     HEA_CUDA(cudaFuncSetAttribute(dt.gen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dt.smem_gen));
     HEA_CUDA(cudaFuncSetAttribute(dt.mc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dt.smem_mc));
 
@@ -405,13 +437,6 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt)
     return HEA_OK;
 }
 
-int choose_block(int tasks)
-{
-    int b = ((tasks + 31) / 32) * 32;
-    if (b > 512) b = 512;
-    return b;
-}
-
 struct DeviceBuf {
     void *p = nullptr;
     ~DeviceBuf()
@@ -429,8 +454,9 @@ struct hea_plan {
     DeviceTables dt;
     hea_params prm{};
     int P = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr, side = nullptr;  // side: the next iteration's new population
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> joins;  // fork/join events between the two streams
     uint8_t *occ = nullptr, *out_occ = nullptr;
     int32_t *cnt = nullptr, *order = nullptr, *scratch = nullptr;
     double *f2 = nullptr, *out_f2 = nullptr;
@@ -440,6 +466,8 @@ struct hea_plan {
     ~hea_plan()
     {
         for (cudaEvent_t e : mc_events) cudaEventDestroy(e);
+        for (cudaEvent_t e : joins) cudaEventDestroy(e);
+        if (side) cudaStreamDestroy(side);
         for (void *p : {(void *)occ, (void *)out_occ, (void *)cnt, (void *)order, (void *)scratch, (void *)f2,
                         (void *)out_f2, (void *)stats})
             if (p) cudaFree(p);
@@ -451,8 +479,10 @@ struct hea_plan {
 
 namespace {
 
-int launch_generate(hea_plan *pl, const int32_t *order, int count, uint32_t generation, int generate)
+int launch_generate(hea_plan *pl, const int32_t *order, int count, uint32_t generation, int generate,
+                    cudaStream_t st = nullptr)
 {
+    if (!st) st = pl->stream;
     GenArgs a{};
     a.nbor = pl->dt.nbor;
     a.occ = pl->occ;
@@ -461,13 +491,14 @@ int launch_generate(hea_plan *pl, const int32_t *order, int count, uint32_t gene
     a.order = order;
     a.generation = generation;
     a.generate = generate;
-    pl->dt.gen<<<count, 512, pl->dt.smem_gen, pl->stream>>>(pl->dt.c, a);
+    pl->dt.gen<<<count, 512, pl->dt.smem_gen, st>>>(pl->dt.c, a);
     HEA_CUDA(cudaGetLastError());
     return HEA_OK;
 }
 
-int launch_mc(hea_plan *pl, const int32_t *order, int count, uint32_t mc_call, McArgs extra)
+int launch_mc(hea_plan *pl, const int32_t *order, int count, uint32_t mc_call, McArgs extra, cudaStream_t st = nullptr)
 {
+    if (!st) st = pl->stream;
     McArgs a = extra;
     a.nbor = pl->dt.nbor;
     a.occ = pl->occ;
@@ -480,11 +511,12 @@ int launch_mc(hea_plan *pl, const int32_t *order, int count, uint32_t mc_call, M
     a.max_rounds = pl->prm.max_rounds > 0 ? pl->prm.max_rounds : (int64_t)1 << 31;
     a.stats = pl->stats;
     const bool timed = (pl->prm.flags & HEA_FLAG_TIME_KERNELS) && 2 * pl->mc_timed + 1 < (int)pl->mc_events.size();
-    if (timed) HEA_CUDA(cudaEventRecord(pl->mc_events[2 * pl->mc_timed], pl->stream));
-    pl->dt.mc<<<count, choose_block(a.tasks), pl->dt.smem_mc, pl->stream>>>(pl->dt.c, a);
+    if (timed) HEA_CUDA(cudaEventRecord(pl->mc_events[2 * pl->mc_timed], st));
+    const int block = choose_block(a.tasks);
+    pl->dt.mc<<<count, block, mc_smem(pl->dt.c.occ_stride, (int)pl->dt.ncount, block / 32), st>>>(pl->dt.c, a);
     HEA_CUDA(cudaGetLastError());
     if (timed) {
-        HEA_CUDA(cudaEventRecord(pl->mc_events[2 * pl->mc_timed + 1], pl->stream));
+        HEA_CUDA(cudaEventRecord(pl->mc_events[2 * pl->mc_timed + 1], st));
         ++pl->mc_timed;
     }
     return HEA_OK;
@@ -501,6 +533,12 @@ int plan_alloc(hea_plan *pl, int slots)
 {
     const SearchConst &c = pl->dt.c;
     HEA_CUDA(cudaStreamCreateWithFlags(&pl->stream, cudaStreamNonBlocking));
+    HEA_CUDA(cudaStreamCreateWithFlags(&pl->side, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+        cudaEvent_t e;
+        HEA_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        pl->joins.push_back(e);
+    }
     HEA_CUDA(cudaEventCreate(&pl->ev0));
     HEA_CUDA(cudaEventCreate(&pl->ev1));
     const size_t occ_bytes = (size_t)slots * c.occ_stride;
@@ -564,10 +602,23 @@ int plan_search(hea_plan *pl, hea_stats *stats)
     HEA_CUDA(cudaGetLastError());
     HEA_CUDA(cudaEventRecord(pl->ev0, pl->stream));
     HEA_TRY(launch_generate(pl, pl->order, P, 0, 1));
-    for (int it = 0; it < pl->prm.total_iter; ++it) {
-        HEA_TRY(launch_generate(pl, pl->order + P, P, (uint32_t)(it + 1), 1));
-        HEA_TRY(launch_mc(pl, pl->order + P, P, (uint32_t)(2 * it), McArgs{}));
+    const int I = pl->prm.total_iter;
+    if (I > 0) {
+        HEA_TRY(launch_generate(pl, pl->order + P, P, 1, 1));
+        HEA_TRY(launch_mc(pl, pl->order + P, P, 0, McArgs{}));
         HEA_TRY(launch_sort(pl, pl->order, 2 * P));
+    }
+    for (int it = 0; it < I; ++it) {
+        // after the merge of iteration it, the new population of iteration it+1
+        // (free slots order[P, 2P)) is generated and searched on the side stream
+        // while the survivors (order[0, P)) are searched on the main stream
+        if (it + 1 < I) {
+            HEA_CUDA(cudaEventRecord(pl->joins[0], pl->stream));
+            HEA_CUDA(cudaStreamWaitEvent(pl->side, pl->joins[0], 0));
+            HEA_TRY(launch_generate(pl, pl->order + P, P, (uint32_t)(it + 2), 1, pl->side));
+            HEA_TRY(launch_mc(pl, pl->order + P, P, (uint32_t)(2 * (it + 1)), McArgs{}, pl->side));
+            HEA_CUDA(cudaEventRecord(pl->joins[1], pl->side));
+        }
         HEA_TRY(launch_mc(pl, pl->order, P, (uint32_t)(2 * it + 1), McArgs{}));
         HEA_TRY(launch_sort(pl, pl->order, P));
         if (pl->prm.flags & HEA_FLAG_LOG_ITERS) {
@@ -578,6 +629,10 @@ int plan_search(hea_plan *pl, hea_stats *stats)
             HEA_CUDA(cudaMemcpyAsync(&best, pl->f2 + best_slot, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
             HEA_CUDA(cudaStreamSynchronize(pl->stream));
             log_iteration(it, std::sqrt(best));
+        }
+        if (it + 1 < I) {
+            HEA_CUDA(cudaStreamWaitEvent(pl->stream, pl->joins[1], 0));
+            HEA_TRY(launch_sort(pl, pl->order, 2 * P));  // merge of iteration it+1
         }
     }
     HEA_CUDA(cudaEventRecord(pl->ev1, pl->stream));
@@ -591,13 +646,29 @@ int plan_search(hea_plan *pl, hea_stats *stats)
         stats->evals = (int64_t)s[1];
         stats->accepts = (int64_t)s[2];
         stats->gpu_ms = ms;
-        stats->mc_ms = 0;
-        stats->mc_launches = pl->mc_timed;
+        // local-search busy time: union of the launch intervals (launches on
+        // the two streams overlap), from event times relative to ev0
+        std::vector<std::pair<float, float>> iv;
         for (int i = 0; i < pl->mc_timed; ++i) {
-            float m = 0;
-            HEA_CUDA(cudaEventElapsedTime(&m, pl->mc_events[2 * i], pl->mc_events[2 * i + 1]));
-            stats->mc_ms += m;
+            float a = 0, b = 0;
+            HEA_CUDA(cudaEventElapsedTime(&a, pl->ev0, pl->mc_events[2 * i]));
+            HEA_CUDA(cudaEventElapsedTime(&b, pl->ev0, pl->mc_events[2 * i + 1]));
+            iv.emplace_back(a, b);
         }
+        std::sort(iv.begin(), iv.end());
+        double busy = 0, lo = 0, hi = -1;
+        for (auto &x : iv) {
+            if (x.first > hi) {
+                if (hi > lo) busy += hi - lo;
+                lo = x.first;
+                hi = x.second;
+            } else if (x.second > hi) {
+                hi = x.second;
+            }
+        }
+        if (hi > lo) busy += hi - lo;
+        stats->mc_ms = busy;
+        stats->mc_launches = pl->mc_timed;
     }
     return HEA_OK;
 }

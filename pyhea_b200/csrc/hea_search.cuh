@@ -1,5 +1,5 @@
 // hea_search.cuh -- the swap-search kernels (sm_100a), templated on the number
-// of species T and of shells S.
+// of species T and on the shell layout of the neighbour table.
 //
 // Layout in HBM (one structure):
 //   nbor   int32 [N][row] with every shell segment padded to a multiple of 4
@@ -27,6 +27,26 @@ struct SearchConst {
     int32_t prefix[kMaxTypes + 1];  // species prefix sums
     int32_t num_sites, row4, occ_stride, num_types, num_shells, feistel_h;
     uint32_t reject_below, key0, key1;
+};
+
+// Shell layout of the padded table, in int4 chunks per shell (0: shell absent).
+// Fixed layouts unroll every load; RuntimeShells reads the chunk counts from
+// SearchConst.
+template <int C0, int C1, int C2>
+struct Shells {
+    static constexpr int S = (C0 > 0) + (C1 > 0) + (C2 > 0);
+    static constexpr bool kRuntime = false;
+    static constexpr int kRow4 = C0 + C1 + C2;
+    __host__ __device__ static constexpr int chunks(int k) { return k == 0 ? C0 : (k == 1 ? C1 : C2); }
+    __host__ __device__ static constexpr int off(int k) { return k == 0 ? 0 : (k == 1 ? C0 : C0 + C1); }
+};
+template <int S_>
+struct RuntimeShells {
+    static constexpr int S = S_;
+    static constexpr bool kRuntime = true;
+    static constexpr int kRow4 = 0;
+    __host__ __device__ static constexpr int chunks(int) { return 0; }
+    __host__ __device__ static constexpr int off(int) { return 0; }
 };
 
 struct AcceptRecord {
@@ -62,8 +82,12 @@ struct GenArgs {
     int32_t generate;  // 1: draw a new occupancy; 0: recount the stored one
 };
 
+__device__ __forceinline__ double inf_d() { return __longlong_as_double(0x7FF0000000000000LL); }
+
 // ---------------------------------------------------------------------------
-// Fitness: f2 = sum_k w_k sum_i sum_j d^2, d = fma(-C', R, E), in k, i, j order.
+// Fitness: f2 = sum_k w_k e_k; e_k accumulates d^2 with fma over the upper
+// triangle row by row (d_ii, then d_ij and d_ji for j > i); d = fma(-C', R, E).
+// Counts are symmetric and R_ij == R_ji, so d_ij and d_ji share C' and R.
 // ---------------------------------------------------------------------------
 template <int T, int S>
 __device__ __forceinline__ double fitness_of_counts(const SearchConst &c, const int32_t *cnt)
@@ -73,36 +97,79 @@ __device__ __forceinline__ double fitness_of_counts(const SearchConst &c, const 
     for (int k = 0; k < S; ++k) {
         double e = 0.0;
 #pragma unroll
-        for (int x = 0; x < T * T; ++x) {
-            const int idx = k * T * T + x;
-            const double d = __fma_rn(-(double)cnt[idx], c.R[idx], c.E[idx]);
-            e = __fma_rn(d, d, e);
+        for (int i = 0; i < T; ++i) {
+            const int ii = (k * T + i) * T + i;
+            const double dii = __fma_rn(-(double)cnt[ii], c.R[ii], c.E[ii]);
+            e = __fma_rn(dii, dii, e);
+#pragma unroll
+            for (int j = i + 1; j < T; ++j) {
+                const int ij = (k * T + i) * T + j, ji = (k * T + j) * T + i;
+                const double cp = (double)cnt[ij];
+                const double dij = __fma_rn(-cp, c.R[ij], c.E[ij]);
+                const double dji = __fma_rn(-cp, c.R[ij], c.E[ji]);
+                e = __fma_rn(dij, dij, e);
+                e = __fma_rn(dji, dji, e);
+            }
         }
         f2 = __fma_rn(c.w[k], e, f2);
     }
     return f2;
 }
 
-// Packed 5-bit species histogram of one padded shell segment of a row, and
-// the number of entries equal to `other`.
-template <bool COUNT_OTHER>
-__device__ __forceinline__ uint32_t segment_hist(const int4 *__restrict__ seg, int chunks, const uint8_t *occ5,
-                                                 uint32_t other, int &m)
+// Packed 5-bit species histogram of four neighbour ids.
+__device__ __forceinline__ uint32_t hist4(const int4 x, const uint8_t *occ5)
 {
-    uint32_t h = 0;
-    for (int ch = 0; ch < chunks; ++ch) {
-        const int4 x = __ldg(seg + ch);
-        h += (1u << occ5[x.x]) + (1u << occ5[x.y]) + (1u << occ5[x.z]) + (1u << occ5[x.w]);
-        if (COUNT_OTHER)
-            m += ((uint32_t)x.x == other) + ((uint32_t)x.y == other) + ((uint32_t)x.z == other) +
-                 ((uint32_t)x.w == other);
-    }
-    return h;
+    return (1u << occ5[x.x]) + (1u << occ5[x.y]) + (1u << occ5[x.z]) + (1u << occ5[x.w]);
 }
 
-// Row/column delta vector u of shell k for swapping species a (at s1) and b
+__device__ __forceinline__ int count4(const int4 x, uint32_t v)
+{
+    return ((uint32_t)x.x == v) + ((uint32_t)x.y == v) + ((uint32_t)x.z == v) + ((uint32_t)x.w == v);
+}
+
+// Histograms of shell k of both rows: h1 (s1's neighbours), h2 (s2's), and m =
+// the number of times s2 appears among s1's neighbours.  Fixed layouts issue
+// every load of the shell (both rows) before the first use.
+template <class L>
+__device__ __forceinline__ void shell_hist(const SearchConst &c, const int4 *__restrict__ r1,
+                                           const int4 *__restrict__ r2, const uint8_t *occ5, uint32_t s2, int k,
+                                           uint32_t &h1, uint32_t &h2, int &m)
+{
+    h1 = 0;
+    h2 = 0;
+    m = 0;
+    if constexpr (L::kRuntime) {
+        const int4 *a = r1 + c.off4[k], *b = r2 + c.off4[k];
+        for (int ch = 0; ch < c.chunks[k]; ++ch) {
+            const int4 x = __ldg(a + ch), y = __ldg(b + ch);
+            h1 += hist4(x, occ5);
+            h2 += hist4(y, occ5);
+            m += count4(x, s2);
+        }
+    } else {
+        constexpr int kMax = 7;
+        int4 x[kMax], y[kMax];
+        const int n = L::chunks(k), o = L::off(k);
+#pragma unroll
+        for (int ch = 0; ch < kMax; ++ch)
+            if (ch < n) {
+                x[ch] = __ldg(r1 + o + ch);
+                y[ch] = __ldg(r2 + o + ch);
+            }
+#pragma unroll
+        for (int ch = 0; ch < kMax; ++ch)
+            if (ch < n) {
+                h1 += hist4(x[ch], occ5);
+                h2 += hist4(y[ch], occ5);
+                m += count4(x[ch], s2);
+            }
+    }
+}
+
+// Row/column delta vector u of a shell for swapping species a (at s1) and b
 // (at s2): u_t = n2_t - n1_t + m([t==b] - [t==a]); the count change is
-// dC_ij = sa_i u_j + sa_j u_i with sa_i = [i==a] - [i==b].
+// dC_ij = sa_i u_j + sa_j u_i with sa_i = [i==a] - [i==b].  Sentinel entries
+// add the same amount to field 0 of h1 and h2 and cancel here.
 template <int T>
 __device__ __forceinline__ void delta_vector(uint32_t h1, uint32_t h2, int m, int a, int b, int (&u)[T])
 {
@@ -113,39 +180,49 @@ __device__ __forceinline__ void delta_vector(uint32_t h1, uint32_t h2, int m, in
     }
 }
 
+// e_k of shell k after adding dC (from u, a, b) to the counts cnt.
+template <int T>
+__device__ __forceinline__ double shell_error(const SearchConst &c, const int32_t *cnt, int k, const int (&u)[T],
+                                              int a, int b)
+{
+    double e = 0.0;
+#pragma unroll
+    for (int i = 0; i < T; ++i) {
+        const int sai = (i == a) - (i == b);
+        const int ii = (k * T + i) * T + i;
+        const double dii = __fma_rn(-(double)(cnt[ii] + 2 * sai * u[i]), c.R[ii], c.E[ii]);
+        e = __fma_rn(dii, dii, e);
+#pragma unroll
+        for (int j = i + 1; j < T; ++j) {
+            const int saj = (j == a) - (j == b);
+            const int ij = (k * T + i) * T + j, ji = (k * T + j) * T + i;
+            const double cp = (double)(cnt[ij] + sai * u[j] + saj * u[i]);
+            const double dij = __fma_rn(-cp, c.R[ij], c.E[ij]);
+            const double dji = __fma_rn(-cp, c.R[ij], c.E[ji]);
+            e = __fma_rn(dij, dij, e);
+            e = __fma_rn(dji, dji, e);
+        }
+    }
+    return e;
+}
+
 // Score one proposal: f2 of the counts after swapping s1 (species a) and s2 (b).
-template <int T, int S>
+// Returns the per-shell histograms so the accept step can apply the change.
+template <int T, class L>
 __device__ __forceinline__ double score_swap(const SearchConst &c, const int4 *__restrict__ nbor, const uint8_t *occ5,
                                              const int32_t *cnt, uint32_t s1, uint32_t s2, int a, int b,
-                                             uint32_t (&h1)[S], uint32_t (&h2)[S], int (&m)[S])
+                                             uint32_t (&h1)[L::S], uint32_t (&h2)[L::S], int (&m)[L::S])
 {
-    const int4 *r1 = nbor + (size_t)s1 * c.row4;
-    const int4 *r2 = nbor + (size_t)s2 * c.row4;
+    const int row4 = L::kRuntime ? c.row4 : L::kRow4;
+    const int4 *r1 = nbor + (size_t)s1 * row4;
+    const int4 *r2 = nbor + (size_t)s2 * row4;
     double f2 = 0.0;
 #pragma unroll
-    for (int k = 0; k < S; ++k) {
-        int mm = 0, unused = 0;
-        const uint32_t H1 = segment_hist<true>(r1 + c.off4[k], c.chunks[k], occ5, s2, mm);
-        const uint32_t H2 = segment_hist<false>(r2 + c.off4[k], c.chunks[k], occ5, 0u, unused);
-        h1[k] = H1;
-        h2[k] = H2;
-        m[k] = mm;
+    for (int k = 0; k < L::S; ++k) {
+        shell_hist<L>(c, r1, r2, occ5, s2, k, h1[k], h2[k], m[k]);
         int u[T];
-        delta_vector<T>(H1, H2, mm, a, b, u);
-        double e = 0.0;
-#pragma unroll
-        for (int i = 0; i < T; ++i) {
-            const int sai = (i == a) - (i == b);
-#pragma unroll
-            for (int j = 0; j < T; ++j) {
-                const int saj = (j == a) - (j == b);
-                const int idx = (k * T + i) * T + j;
-                const int cp = cnt[idx] + sai * u[j] + saj * u[i];
-                const double d = __fma_rn(-(double)cp, c.R[idx], c.E[idx]);
-                e = __fma_rn(d, d, e);
-            }
-        }
-        f2 = __fma_rn(c.w[k], e, f2);
+        delta_vector<T>(h1[k], h2[k], m[k], a, b, u);
+        f2 = __fma_rn(c.w[k], shell_error<T>(c, cnt, k, u, a, b), f2);
     }
     return f2;
 }
@@ -172,8 +249,6 @@ __device__ __forceinline__ bool draw_pair(const SearchConst &c, uint32_t stream,
     }
     return false;
 }
-
-__device__ __forceinline__ double inf_d() { return __longlong_as_double(0x7FF0000000000000LL); }
 
 // Lexicographic (f2, task) minimum: the lowest task wins ties.
 __device__ __forceinline__ bool better(double f, int q, double bf, int bq) { return f < bf || (f == bf && q < bq); }
@@ -292,31 +367,53 @@ __global__ void __launch_bounds__(512, 1) generate_kernel(const SearchConst c, c
 
 // ---------------------------------------------------------------------------
 // The local parallel search (pyhea/cpp/accelerate.cpp:601-694): one CTA per
-// solution, one thread per task (threads loop when tasks > blockDim).  Each
-// round every task scores one proposal against the same state; the block takes
-// the (f2, task) minimum and accepts it iff it is strictly below the current
-// f2; the search ends after `depth` rounds in a row without an accept.
-// Dynamic shared memory = occ_stride + 16 + 4*S*T*T + 32*(8+4) + 16 bytes.
+// solution, one lane per task (lanes loop when tasks > blockDim).  Each round
+// every task scores one proposal against the same state; the block takes the
+// (f2, task) minimum and accepts it iff it is strictly below the current f2;
+// the search ends after `depth` rounds in a row without an accept.
+//
+// One block barrier per round: each warp publishes its best proposal (a
+// SwapRecord, double-buffered by round parity) before the barrier; after it
+// every warp reduces the records itself, writes the winning swap into the
+// shared occupancy (all threads write the same two bytes) and applies the count
+// change to its own copy of the counts, so no second barrier is needed before
+// the next round reads them.
+// Dynamic shared memory: occ_stride + 16 + nwarps * 4 * ncount_pad + 2 * 32 * sizeof(SwapRecord).
 // ---------------------------------------------------------------------------
-template <int T, int S>
-__global__ void __launch_bounds__(512, 1) mc_kernel(const SearchConst c, const McArgs g)
-{
-    extern __shared__ __align__(16) uint8_t smem[];
-    uint8_t *occ5 = smem;
-    int32_t *cnt = reinterpret_cast<int32_t *>(smem + c.occ_stride + 16);
-    double *red_f = reinterpret_cast<double *>(cnt + ((S * T * T + 3) & ~3));
-    int *red_q = reinterpret_cast<int *>(red_f + 32);
-    double *ctl_f = reinterpret_cast<double *>(red_q + 32);
-    int *ctl_q = reinterpret_cast<int *>(ctl_f + 1);
+struct SwapRecord {
+    double f2;
+    int32_t task;
+    uint32_t s1, s2;
+    int32_t ab;          // species a | b << 8 before the swap
+    uint32_t h1[3], h2[3];
+    int32_t m;           // m_k in byte k
+    int32_t pad_;
+};
+static_assert(sizeof(SwapRecord) == 56, "SwapRecord layout");
 
+__host__ __device__ constexpr int mc_ncount_pad(int ncount) { return (ncount + 3) & ~3; }
+
+#ifndef HEA_MC_MIN_BLOCKS
+#define HEA_MC_MIN_BLOCKS 2  // resident 512-thread blocks per SM the register budget aims for
+#endif
+template <int T, class L>
+__global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const SearchConst c, const McArgs g)
+{
+    constexpr int S = L::S, NC = S * T * T, NCP = mc_ncount_pad(NC);
+    extern __shared__ __align__(16) uint8_t smem[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    uint8_t *occ5 = smem;
+    int32_t *cnt_all = reinterpret_cast<int32_t *>(smem + c.occ_stride + 16);
+    int32_t *cnt = cnt_all + warp * NCP;  // this warp's copy of the counts
+    SwapRecord *rec = reinterpret_cast<SwapRecord *>(cnt_all + nwarps * NCP);  // [2][32]
+
     const int slot = g.order[blockIdx.x];
     const uint32_t stream = (g.mc_call << 16) | (uint32_t)blockIdx.x;
     uint8_t *gocc = g.occ + (size_t)slot * c.occ_stride;
-    int32_t *gcnt = g.cnt + (size_t)slot * S * T * T;
+    int32_t *gcnt = g.cnt + (size_t)slot * NC;
     const int n = c.num_sites;
 
-    {  // stage the slot: occupancy as 5*species (16-byte vectors), counts
+    {  // stage the slot: occupancy as 5*species (16-byte vectors), counts per warp
         const uint4 *src = reinterpret_cast<const uint4 *>(gocc);
         uint4 *dst = reinterpret_cast<uint4 *>(occ5);
         for (int v = tid; v < c.occ_stride / 16; v += blockDim.x) {
@@ -325,7 +422,7 @@ __global__ void __launch_bounds__(512, 1) mc_kernel(const SearchConst c, const M
             x.x = x.x * 5u; x.y = x.y * 5u; x.z = x.z * 5u; x.w = x.w * 5u;
             dst[v] = x;
         }
-        for (int x = tid; x < S * T * T; x += blockDim.x) cnt[x] = gcnt[x];
+        for (int x = lane; x < NC; x += 32) cnt[x] = gcnt[x];
     }
     __syncthreads();
     if (tid == 0) occ5[n] = 0;  // sentinel (occ_stride may end exactly at n)
@@ -335,91 +432,107 @@ __global__ void __launch_bounds__(512, 1) mc_kernel(const SearchConst c, const M
     int miss = 0;
     int64_t round = 0, accepts = 0, evals = 0;
     while (miss < g.depth && round < g.max_rounds) {
-        double bf = inf_d();  // +inf
-        int bq = 0x7FFFFFFF;
-        uint32_t b1 = 0, b2 = 0, bh1[S], bh2[S];
-        int bm[S];
-        for (int q = tid; q < g.tasks; q += blockDim.x) {
-            uint32_t s1, s2;
-            if (!draw_pair(c, stream, (uint32_t)round, (uint32_t)q, occ5, s1, s2)) continue;
-            ++evals;
-            uint32_t h1[S], h2[S];
-            int m[S];
-            const double f = score_swap<T, S>(c, g.nbor, occ5, cnt, s1, s2, occ5[s1] / 5, occ5[s2] / 5, h1, h2, m);
-            if (f < bf) {
-                bf = f;
-                bq = q;
-                b1 = s1;
-                b2 = s2;
-#pragma unroll
-                for (int k = 0; k < S; ++k) {
-                    bh1[k] = h1[k];
-                    bh2[k] = h2[k];
-                    bm[k] = m[k];
-                }
-            }
-        }
-        double wf = bf;
-        int wq = bq;
-        warp_argmin(wf, wq);
+        SwapRecord *rr = rec + (round & 1) * 32;
+        SwapRecord &mine = rr[warp];  // this warp's best proposal of the round
         if (lane == 0) {
-            red_f[warp] = wf;
-            red_q[warp] = wq;
+            mine.f2 = inf_d();
+            mine.task = 0x7FFFFFFF;
+        }
+        __syncwarp();
+        // passes of blockDim tasks; lane q of a pass scores task q (warp-uniform trip count)
+        for (int q0 = warp * 32; q0 < g.tasks; q0 += blockDim.x) {
+            const int q = q0 + lane;
+            uint32_t s1 = 0, s2 = 0;
+            const bool ok = q < g.tasks && draw_pair(c, stream, (uint32_t)round, (uint32_t)q, occ5, s1, s2);
+            __syncwarp();  // lanes that needed more draws rejoin before scoring
+            double f = inf_d();
+            uint32_t h1[S], h2[S];
+            int m[S], a = 0, b = 0;
+            if (ok) {
+                ++evals;
+                a = occ5[s1] / 5;
+                b = occ5[s2] / 5;
+                f = score_swap<T, L>(c, g.nbor, occ5, cnt, s1, s2, a, b, h1, h2, m);
+            }
+            double wf = f;
+            int wq = ok ? q : 0x7FFFFFFF;
+            warp_argmin(wf, wq);
+            // the lane holding the pass minimum folds it into the warp's record
+            if (ok && wq == q && better(wf, wq, mine.f2, mine.task)) {
+                SwapRecord r;
+                r.f2 = wf;
+                r.task = wq;
+                r.s1 = s1;
+                r.s2 = s2;
+                r.ab = a | (b << 8);
+                r.m = 0;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    r.h1[k] = k < S ? h1[k < S ? k : 0] : 0;
+                    r.h2[k] = k < S ? h2[k < S ? k : 0] : 0;
+                    if (k < S) r.m |= m[k < S ? k : 0] << (8 * k);
+                }
+                r.pad_ = 0;
+                mine = r;
+            }
+            __syncwarp();
         }
         __syncthreads();
-        if (warp == 0) {
-            double xf = lane < nwarps ? red_f[lane] : inf_d();
-            int xq = lane < nwarps ? red_q[lane] : 0x7FFFFFFF;
-            warp_argmin(xf, xq);
-            if (lane == 0) {
-                *ctl_f = xf;
-                *ctl_q = xq;
+        // every warp reduces the records of all warps
+        double xf = lane < nwarps ? rr[lane].f2 : inf_d();
+        int xq = lane < nwarps ? rr[lane].task : 0x7FFFFFFF;
+        int xw = lane;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const double of = __shfl_xor_sync(0xFFFFFFFFu, xf, o);
+            const int oq = __shfl_xor_sync(0xFFFFFFFFu, xq, o);
+            const int ow = __shfl_xor_sync(0xFFFFFFFFu, xw, o);
+            if (better(of, oq, xf, xq)) {
+                xf = of;
+                xq = oq;
+                xw = ow;
             }
         }
-        __syncthreads();
-        const double win_f = *ctl_f;
-        const int win_q = *ctl_q;
-        if (win_f < cur) {
-            if (bq == win_q) {  // this thread owns the winning proposal
-                const int a = occ5[b1] / 5, b = occ5[b2] / 5;
-                const uint8_t t = occ5[b1];
-                occ5[b1] = occ5[b2];
-                occ5[b2] = t;
-#pragma unroll
-                for (int k = 0; k < S; ++k) {
-                    int u[T];
-                    delta_vector<T>(bh1[k], bh2[k], bm[k], a, b, u);
-#pragma unroll
-                    for (int j = 0; j < T; ++j) {
-                        cnt[(k * T + a) * T + j] += u[j];
-                        cnt[(k * T + j) * T + a] += u[j];
-                        cnt[(k * T + b) * T + j] -= u[j];
-                        cnt[(k * T + j) * T + b] -= u[j];
-                    }
-                }
-                if (g.trace && accepts < g.trace_cap) {
+        if (xf < cur) {
+            const SwapRecord &w = rr[xw];
+            const int a = w.ab & 0xFF, b = (w.ab >> 8) & 0xFF;
+            occ5[w.s1] = (uint8_t)(5 * b);  // same bytes from every thread
+            occ5[w.s2] = (uint8_t)(5 * a);
+            for (int x = lane; x < NC; x += 32) {
+                const int k = x / (T * T), i = (x / T) % T, j = x % T;
+                const uint32_t h1 = w.h1[k], h2 = w.h2[k];
+                const int m = (w.m >> (8 * k)) & 0xFF;
+                const int ui = (int)((h2 >> (5 * i)) & 31u) - (int)((h1 >> (5 * i)) & 31u) + (i == b ? m : 0) -
+                               (i == a ? m : 0);
+                const int uj = (int)((h2 >> (5 * j)) & 31u) - (int)((h1 >> (5 * j)) & 31u) + (j == b ? m : 0) -
+                               (j == a ? m : 0);
+                cnt[x] += ((i == a) - (i == b)) * uj + ((j == a) - (j == b)) * ui;
+            }
+            __syncwarp();
+            if (g.trace && warp == 0 && accepts < g.trace_cap) {
+                if (lane == 0) {
                     AcceptRecord r;
                     r.round = (uint32_t)round;
-                    r.task = (uint32_t)win_q;
-                    r.s1 = b1;
-                    r.s2 = b2;
-                    r.f2 = win_f;
+                    r.task = (uint32_t)xq;
+                    r.s1 = w.s1;
+                    r.s2 = w.s2;
+                    r.f2 = xf;
                     g.trace[(size_t)blockIdx.x * g.trace_cap + accepts] = r;
-                    if (g.trace_counts) {
-                        int32_t *dst = g.trace_counts + ((size_t)blockIdx.x * g.trace_cap + accepts) * S * T * T;
-                        for (int x = 0; x < S * T * T; ++x) dst[x] = cnt[x];
-                    }
+                }
+                if (g.trace_counts) {
+                    int32_t *dst = g.trace_counts + ((size_t)blockIdx.x * g.trace_cap + accepts) * NC;
+                    for (int x = lane; x < NC; x += 32) dst[x] = cnt[x];
                 }
             }
-            cur = win_f;
+            cur = xf;
             miss = 0;
             ++accepts;
-            __syncthreads();
         } else {
             ++miss;
         }
         ++round;
     }
+    __syncthreads();
 
     // write the slot back
     {
@@ -441,7 +554,8 @@ __global__ void __launch_bounds__(512, 1) mc_kernel(const SearchConst c, const M
             }
             dst[v] = make_uint4(o[0], o[1], o[2], o[3]);
         }
-        for (int x = tid; x < S * T * T; x += blockDim.x) gcnt[x] = cnt[x];
+        if (warp == 0)
+            for (int x = lane; x < NC; x += 32) gcnt[x] = cnt[x];
     }
     // evals per thread -> block total
     unsigned long long ev = (unsigned long long)evals;
