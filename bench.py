@@ -208,10 +208,10 @@ def main():
     nbor, sizes = st.neighbors(device=True)
     plan = hb.Plan(problem, st.P, st.I, st.Q, st.D, time_kernels=True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    base = 1_000_003 * rank
+    from pyhea_b200 import replicas
 
     for w in range(args.warmup):
-        plan.run(base + w)
+        plan.run(replicas.replica_seed(rank, w))
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -222,7 +222,7 @@ def main():
     for k in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
-        s = plan.run(base + args.warmup + k)
+        s = plan.run(replicas.replica_seed(rank, args.warmup + k))
         total_ms += s["gpu_ms"]
         evals += s["evals"]
         mc_ms += s["mc_ms"]
@@ -244,20 +244,17 @@ def main():
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        _, _, s = hb.search(hp, st.P, st.I, st.Q, st.D, seed=base + 7_777 + k, out_occ=out_occ, out_fitness=out_fit)
+        _, _, s = hb.search(hp, st.P, st.I, st.Q, st.D, seed=replicas.replica_seed(rank, 10_000 + k), out_occ=out_occ,
+                            out_fitness=out_fit)
         e2e_s += time.perf_counter() - t0
         e2e_evals += s["evals"]
     h2d = (hp.nbor.nbytes + hp.shell_sizes.nbytes + hp.species.nbytes + hp.weight.nbytes + hp.target_sro.nbytes)
     d2h = out_occ.nbytes + out_fit.nbytes
 
-    if dist:
-        t = torch.tensor([total_ms, float(evals), e2e_s, float(e2e_evals)], dtype=torch.float64, device="cuda")
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        total_ms_max, evals_all, e2e_max, e2e_evals_all = tmax[0].item(), t[1].item(), tmax[2].item(), t[3].item()
-    else:
-        total_ms_max, evals_all, e2e_max, e2e_evals_all = total_ms, float(evals), e2e_s, float(e2e_evals)
+    dev = torch.device("cuda", local)
+    total_ms_max, evals_all = replicas.combine(total_ms, evals, device=dev)
+    e2e_ms_max, e2e_evals_all = replicas.combine(1000.0 * e2e_s, e2e_evals, device=dev)
+    e2e_max = e2e_ms_max / 1000.0
 
     if rank == 0:
         peak, peak_kind = measured_peaks()

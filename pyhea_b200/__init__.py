@@ -10,7 +10,7 @@ Two front ends over one CUDA library (libhea_cuda.so, C ABI in include/hea_cuda.
   ``build_neighbors``), used by the tests and the benchmark.
 
 Importing the package loads the CUDA library and raises ImportError when it has
-not been built (``python -m pyhea_b200.build``); there is no CPU fallback.
+not been built (``python pyhea_b200/build.py``); there is no CPU fallback.
 """
 import ctypes
 import os
@@ -20,7 +20,7 @@ import numpy as np
 _PKG = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_PKG, "libhea_cuda.so")
 if not os.path.exists(_LIB_PATH):
-    raise ImportError(f"{_LIB_PATH} is missing; build it with `python -m pyhea_b200.build`")
+    raise ImportError(f"{_LIB_PATH} is missing; build it with `python pyhea_b200/build.py`")
 
 _P = ctypes.POINTER
 _i32, _i64, _u32, _u64, _f64, _u8 = (ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32, ctypes.c_uint64,

@@ -4,7 +4,7 @@
   pyhea_b200/accelerate<ext-suffix> pybind11 module `accelerate`, the drop-in for
                                     pyhea.cpp.accelerate; links libhea_cuda.so
 
-Run `python -m pyhea_b200.build` (or __graft_entry__.build()).  Objects are
+Run `python pyhea_b200/build.py` (or __graft_entry__.build()).  Objects are
 rebuilt when a source is newer than the library.
 """
 import glob
