@@ -125,6 +125,24 @@ int hea_local_search(const hea_problem *problem, uint64_t seed, uint32_t mc_call
                      int64_t *trace_len);
 
 /*
+ * Allocation-free form of hea_recount (same arguments, same results).  It has
+ * no counterpart in the reference.  It is for callers that cannot allocate
+ * device memory -- a process whose GPU memory is reserved up front by another
+ * allocator, or code that must not trigger cudaMalloc's device-wide
+ * synchronisation -- and it never calls cudaMalloc or cudaFree: all its device
+ * buffers live in one static device array of HEA_NOALLOC_SCRATCH_BYTES, which
+ * every GPU that loads the library holds until the process exits.  The first
+ * call on a device looks up that array's address (once per device, with the
+ * device current); make it before any stream capture.  Inputs whose raw and
+ * padded neighbour tables plus `count` occupancy rows, counts and f2 exceed
+ * the array are rejected with HEA_ERR_UNSUPPORTED.  All calls share the array:
+ * calls that overlap on the GPU (from two host threads) race.
+ */
+#define HEA_NOALLOC_SCRATCH_BYTES (16u << 20)
+int hea_recount_noalloc(const hea_problem *problem, int32_t count, const uint8_t *occ, int32_t *out_counts,
+                        double *out_f2);
+
+/*
  * Neighbour table of a perfect cubic supercell built on the device, in the
  * site numbering and shell order of pyhea/lattice/lattice.py:146-323
  * (ids sorted within each shell).  lattice: 0 = FCC, 1 = BCC.  shell_set:

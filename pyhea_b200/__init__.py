@@ -82,6 +82,7 @@ def _declare(lib):
         "hea_local_search": (_i32, [_P(_Problem), _u64, _u32, _i32, _i32, _i32, _i64, _P(_u8), _P(_i32), _P(_f64),
                                     _P(_i64), _P(AcceptRecord), _P(_i32), _i64, _P(_i64)]),
         "hea_build_neighbors": (_i32, [_i32, _i32, _i32, _P(_i32), _P(_i32), _P(_i32)]),
+        "hea_recount_noalloc": (_i32, [_P(_Problem), _i32, _P(_u8), _P(_i32), _P(_f64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -233,6 +234,19 @@ def local_search(problem, seed, mc_call, occ, tasks, depth, max_rounds=0, trace_
         out["trace_len"] = tlen
         out["trace_counts"] = tc
     return out
+
+
+def recount_noalloc(problem, occ):
+    """hea_recount_noalloc: the same results as recount() from a fixed static
+    device array instead of allocated buffers (for callers that cannot
+    allocate device memory)."""
+    occ = np.ascontiguousarray(np.atleast_2d(occ), dtype=np.uint8)
+    count = occ.shape[0]
+    cnt = np.empty((count, problem.num_shells, problem.num_types, problem.num_types), dtype=np.int32)
+    f2 = np.empty(count)
+    _check(lib.hea_recount_noalloc(ctypes.byref(problem._c), int(count), _ptr(occ, _u8), _ptr(cnt, _i32),
+                                   _ptr(f2, _f64)))
+    return cnt, f2
 
 
 def build_neighbors(lattice, cell, shell_set=SHELLS_REFERENCE):

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstring>
 #include <ctime>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -913,3 +914,168 @@ int hea_build_neighbors(int32_t lattice, int32_t cell, int32_t shell_set, int32_
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free recount (hea_recount_noalloc).
+//
+// For callers that cannot allocate device memory: processes whose device
+// memory is fully reserved by another allocator (a framework's caching pool
+// that claims the GPU at start-up), or code that must not pay cudaMalloc's
+// implicit device-wide synchronisation.  Every device buffer the recount needs
+// (raw and padded neighbour table, occupancy rows, slot order, counts, f2,
+// error flag) is carved out of one fixed static array; nothing is allocated
+// or freed.  The array is shared by all calls and keeps the previous call's
+// contents: the error flag is cleared and the counts are rebuilt from zero on
+// every call.  Two calls that overlap on the GPU (two host threads, or a call
+// while another is still running) race on the array.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[HEA_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device with that device current.
+int noalloc_scratch(void **out)
+{
+    int dev = 0;
+    HEA_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(HEA_ERR_UNSUPPORTED, "device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        HEA_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return HEA_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" int hea_recount_noalloc(const hea_problem *problem, int32_t count, const uint8_t *occ, int32_t *out_counts,
+                                   double *out_f2)
+{
+    if (count < 1 || count > 65535) return fail(HEA_ERR_INVALID, "count must be 1..65535");
+    if (!occ || !out_counts || !out_f2) return fail(HEA_ERR_INVALID, "occ, out_counts and out_f2 must not be NULL");
+    HEA_TRY(validate_problem(problem));
+    const hea_problem *pb = problem;
+    const int T = pb->num_types, S = pb->num_shells, N = pb->num_sites;
+    const int ncount = S * T * T;
+
+    // the recount's constants (fitness tables, padded shell geometry)
+    SearchConst c;
+    std::memset(&c, 0, sizeof(c));
+    PadGeom g{};
+    int raw_row = 0, poff = 0;
+    for (int k = 0; k < S; ++k) {
+        const int z = pb->shell_sizes[k], zp = (z + 3) & ~3;
+        g.size[k] = z;
+        g.off[k] = raw_row;
+        g.poff[k] = poff;
+        g.psize[k] = zp;
+        c.off4[k] = poff / 4;
+        c.chunks[k] = zp / 4;
+        c.pad[k] = zp - z;
+        raw_row += z;
+        poff += zp;
+    }
+    g.num_shells = S;
+    g.raw_row = raw_row;
+    g.pad_row = poff;
+    g.num_sites = N;
+    c.row4 = poff / 4;
+    c.num_sites = N;
+    c.num_types = T;
+    c.num_shells = S;
+    c.occ_stride = (N + 15) & ~15;
+    c.prefix[0] = 0;
+    for (int t = 0; t < T; ++t) c.prefix[t + 1] = c.prefix[t] + pb->species[t];
+    for (int k = 0; k < S; ++k) {
+        c.w[k] = pb->weight[k];
+        for (int i = 0; i < T; ++i)
+            for (int j = 0; j < T; ++j) {
+                const int e = (k * T + i) * T + j;
+                c.E[e] = 1.0 - pb->target_sro[(size_t)k * T * T + i * T + j];
+                c.R[e] = (double)N / (((double)pb->shell_sizes[k] * (double)pb->species[i]) * (double)pb->species[j]);
+            }
+    }
+    // occupancies must hold the problem's composition
+    for (int p = 0; p < count; ++p) {
+        int64_t h[kMaxTypes] = {};
+        for (int s = 0; s < N; ++s) {
+            const uint8_t v = occ[(size_t)p * N + s];
+            if (v >= T) return fail(HEA_ERR_INVALID, "occupancy holds species %d >= %d", v, T);
+            ++h[v];
+        }
+        for (int t = 0; t < T; ++t)
+            if (h[t] != c.prefix[t + 1] - c.prefix[t])
+                return fail(HEA_ERR_INVALID, "occupancy %d has %lld atoms of species %d, element says %d", p,
+                            (long long)h[t], t, c.prefix[t + 1] - c.prefix[t]);
+    }
+
+    // scratch layout
+    const size_t raw_bytes = (size_t)N * raw_row * sizeof(int32_t);
+    const size_t pad_bytes = (size_t)N * poff * sizeof(int32_t);
+    const size_t o_raw = 0;
+    const size_t o_pad = align256(o_raw + raw_bytes);
+    const size_t o_occ = align256(o_pad + pad_bytes);
+    const size_t o_cnt = align256(o_occ + (size_t)count * c.occ_stride);
+    const size_t o_f2 = align256(o_cnt + (size_t)count * ncount * sizeof(int32_t));
+    const size_t o_order = align256(o_f2 + (size_t)count * sizeof(double));
+    const size_t o_err = align256(o_order + (size_t)count * sizeof(int32_t));
+    const size_t need = o_err + sizeof(int);
+    if (need > (size_t)HEA_NOALLOC_SCRATCH_BYTES)
+        return fail(HEA_ERR_UNSUPPORTED,
+                    "%d sites x %d occupancies need %zu bytes of scratch; the allocation-free recount has %zu "
+                    "(HEA_NOALLOC_SCRATCH_BYTES)",
+                    N, count, need, (size_t)HEA_NOALLOC_SCRATCH_BYTES);
+    const size_t smem = (size_t)c.occ_stride + 16 + 4 * (size_t)((ncount + 3) & ~3);
+    if (smem > (size_t)smem_limit())
+        return fail(HEA_ERR_UNSUPPORTED, "%d sites need %zu bytes of shared memory, above the %d-byte limit", N, smem,
+                    smem_limit());
+
+    void *base = nullptr;
+    HEA_TRY(noalloc_scratch(&base));
+    unsigned char *sc = static_cast<unsigned char *>(base);
+    int32_t *d_raw = reinterpret_cast<int32_t *>(sc + o_raw);
+    int32_t *d_pad = reinterpret_cast<int32_t *>(sc + o_pad);
+    uint8_t *d_occ = sc + o_occ;
+    int32_t *d_cnt = reinterpret_cast<int32_t *>(sc + o_cnt);
+    double *d_f2 = reinterpret_cast<double *>(sc + o_f2);
+    int32_t *d_order = reinterpret_cast<int32_t *>(sc + o_order);
+    int *d_err = reinterpret_cast<int *>(sc + o_err);
+
+    const GenFn gen = kGen[T][S];
+    HEA_CUDA(cudaFuncSetAttribute(gen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HEA_CUDA(cudaMemcpy(d_raw, pb->nbor, raw_bytes, cudaMemcpyHostToDevice));
+    HEA_CUDA(cudaMemset(d_err, 0, sizeof(int)));
+    pad_and_check_kernel<<<1184, 256>>>(d_raw, d_pad, g, d_err);
+    HEA_CUDA(cudaGetLastError());
+    int herr = 0;
+    HEA_CUDA(cudaMemcpy(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr & 1) return fail(HEA_ERR_INVALID, "neighbour list holds an id outside [0, %d)", N);
+    if (herr & 2) return fail(HEA_ERR_UNSUPPORTED, "neighbour list names a site as its own neighbour");
+    if (herr & 4) return fail(HEA_ERR_UNSUPPORTED, "neighbour list is not symmetric within a shell");
+    HEA_CUDA(cudaMemcpy2D(d_occ, c.occ_stride, occ, N, N, count, cudaMemcpyHostToDevice));
+    iota_kernel<<<(count + 255) / 256, 256>>>(d_order, count);
+    HEA_CUDA(cudaGetLastError());
+    GenArgs a{};
+    a.nbor = reinterpret_cast<const int4 *>(d_pad);
+    a.occ = d_occ;
+    a.cnt = d_cnt;
+    a.f2 = d_f2;
+    a.order = d_order;
+    a.generation = 0;
+    a.generate = 0;
+    gen<<<count, 512, smem>>>(c, a);
+    HEA_CUDA(cudaGetLastError());
+    HEA_CUDA(cudaMemcpy(out_counts, d_cnt, (size_t)count * ncount * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    HEA_CUDA(cudaMemcpy(out_f2, d_f2, (size_t)count * sizeof(double), cudaMemcpyDeviceToHost));
+    return HEA_OK;
+}
