@@ -103,6 +103,24 @@ int hea_plan_read(hea_plan *plan, uint8_t *out_occ, double *out_fitness);
 void hea_plan_destroy(hea_plan *plan);
 
 /*
+ * Batched search: `count` independent structures (each with its own problem,
+ * parameters and seed) searched together by one persistent kernel, the run
+ * captured once as a CUDA graph.  Each structure's result is identical to
+ * hea_run_local_parallel_hcs on that structure alone with the same seed.
+ * There is no counterpart in the reference, which searches one structure per
+ * call (accelerate.cu:1112-1242); this batches many such calls.
+ * run: seeds [count] (NULL keeps the previous ones); read: structure index's
+ * occupancies [P][N] and fitness [P], ascending.
+ */
+typedef struct hea_batch hea_batch;
+int hea_batch_create(const hea_problem *problems, const hea_params *params, int32_t count, hea_batch **out);
+int hea_batch_run(hea_batch *batch, const uint64_t *seeds, hea_stats *stats);
+int hea_batch_read(hea_batch *batch, int32_t index, uint8_t *out_occ, double *out_fitness);
+/* Milliseconds from the start of the last run to each structure's final sort (device clock). */
+int hea_batch_finish_times(hea_batch *batch, double *out_ms);
+void hea_batch_destroy(hea_batch *batch);
+
+/*
  * Component entry points (host buffers), one launch each, used to check the
  * pieces of the search against the CPU restatement.
  *

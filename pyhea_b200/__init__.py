@@ -83,6 +83,11 @@ def _declare(lib):
                                     _P(_i64), _P(AcceptRecord), _P(_i32), _i64, _P(_i64)]),
         "hea_build_neighbors": (_i32, [_i32, _i32, _i32, _P(_i32), _P(_i32), _P(_i32)]),
         "hea_recount_noalloc": (_i32, [_P(_Problem), _i32, _P(_u8), _P(_i32), _P(_f64)]),
+        "hea_batch_create": (_i32, [_P(_Problem), _P(_Params), _i32, _P(ctypes.c_void_p)]),
+        "hea_batch_run": (_i32, [ctypes.c_void_p, _P(_u64), _P(Stats)]),
+        "hea_batch_read": (_i32, [ctypes.c_void_p, _i32, _P(_u8), _P(_f64)]),
+        "hea_batch_finish_times": (_i32, [ctypes.c_void_p, _P(_f64)]),
+        "hea_batch_destroy": (None, [ctypes.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -179,6 +184,53 @@ class Plan:
     def close(self):
         if self._h:
             lib.hea_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many structures searched together by one persistent kernel (hea_batch_*).
+
+    problems: list of Problem; params: list of dicts with num_solutions,
+    total_iter, parallel_task, converge_depth (and optional max_rounds).  Each
+    structure's result equals search() on it alone with the same seed."""
+
+    def __init__(self, problems, params):
+        self.problems = list(problems)
+        n = len(self.problems)
+        self._pb = (_Problem * n)(*[p._c for p in self.problems])
+        self._prm = (_Params * n)(*[_params(q["num_solutions"], q["total_iter"], q["parallel_task"],
+                                            q["converge_depth"], 0, q.get("max_rounds", 0)) for q in params])
+        self.P = [int(q["num_solutions"]) for q in params]
+        self._h = ctypes.c_void_p()
+        _check(lib.hea_batch_create(self._pb, self._prm, n, ctypes.byref(self._h)))
+
+    def run(self, seeds):
+        arr = (_u64 * len(self.problems))(*[int(s) & 0xFFFFFFFFFFFFFFFF for s in seeds])
+        st = Stats()
+        _check(lib.hea_batch_run(self._h, arr, ctypes.byref(st)))
+        return st.as_dict()
+
+    def read(self, index):
+        occ = np.empty((self.P[index], self.problems[index].num_sites), dtype=np.uint8)
+        fit = np.empty(self.P[index], dtype=np.float64)
+        _check(lib.hea_batch_read(self._h, int(index), _ptr(occ, _u8), _ptr(fit, _f64)))
+        return occ, fit
+
+    def finish_times(self):
+        """Milliseconds from the start of the last run to each structure's end."""
+        out = np.empty(len(self.problems))
+        _check(lib.hea_batch_finish_times(self._h, _ptr(out, _f64)))
+        return out
+
+    def close(self):
+        if self._h:
+            lib.hea_batch_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

@@ -333,7 +333,7 @@ int smem_limit()
 
 size_t mc_smem(int occ_stride, int ncount, int nwarps)
 {
-    return (size_t)occ_stride + 16 + (size_t)nwarps * 4 * mc_ncount_pad(ncount) + 2 * 32 * sizeof(SwapRecord);
+    return (size_t)occ_stride + 16 + (size_t)nwarps * (4 * mc_ncount_pad(ncount) + 2 * sizeof(SwapRecord));
 }
 
 int choose_block(int tasks)
@@ -341,6 +341,18 @@ int choose_block(int tasks)
     int b = ((tasks + 31) / 32) * 32;
     if (b > 512) b = 512;
     return b;
+}
+
+// Kernels are shared by every plan and batch: allow them the device's largest
+// dynamic shared memory (the opt-in limit less their static shared memory),
+// never one plan's size.
+template <class F>
+cudaError_t allow_max_smem(F *func)
+{
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, func);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_limit() - (int)a.sharedSizeBytes);
 }
 
 int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt)
@@ -405,8 +417,8 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt)
                     N, dt.smem_mc, smem_limit());
     dt.gen = kGen[T][S];
     dt.mc = pick_mc(T, c.chunks[0], S > 1 ? c.chunks[1] : 0, S > 2 ? c.chunks[2] : 0, S);
-    HEA_CUDA(cudaFuncSetAttribute(dt.gen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dt.smem_gen));
-    HEA_CUDA(cudaFuncSetAttribute(dt.mc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dt.smem_mc));
+    HEA_CUDA(allow_max_smem(dt.gen));
+    HEA_CUDA(allow_max_smem(dt.mc));
 
     // padded table on the device, checked
     const size_t raw_bytes = (size_t)N * raw_row * sizeof(int32_t);
@@ -1052,7 +1064,7 @@ extern "C" int hea_recount_noalloc(const hea_problem *problem, int32_t count, co
     int *d_err = reinterpret_cast<int *>(sc + o_err);
 
     const GenFn gen = kGen[T][S];
-    HEA_CUDA(cudaFuncSetAttribute(gen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HEA_CUDA(allow_max_smem(gen));
     HEA_CUDA(cudaMemcpy(d_raw, pb->nbor, raw_bytes, cudaMemcpyHostToDevice));
     HEA_CUDA(cudaMemset(d_err, 0, sizeof(int)));
     pad_and_check_kernel<<<1184, 256>>>(d_raw, d_pad, g, d_err);
@@ -1079,3 +1091,272 @@ extern "C" int hea_recount_noalloc(const hea_problem *problem, int32_t count, co
     HEA_CUDA(cudaMemcpy(out_f2, d_f2, (size_t)count * sizeof(double), cudaMemcpyDeviceToHost));
     return HEA_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batched search: many structures in one persistent kernel (hea_batch.cuh)
+// ---------------------------------------------------------------------------
+#include "hea_batch.cuh"
+
+struct hea_batch {
+    int count = 0;
+    std::vector<DeviceTables *> tables;
+    std::vector<BatchStruct> h_structs;
+    std::vector<void *> buffers;  // every device allocation of the batch
+    BatchStruct *d_structs = nullptr;
+    BatchState *d_states = nullptr;
+    BatchJob *d_jobs = nullptr;
+    BatchCtl *d_ctl = nullptr;
+    unsigned long long *d_finish = nullptr;  // per structure: ns from start to its last sort
+    unsigned long long total_jobs = 0;
+    size_t smem = 0;
+    int grid = 0, block = HEA_BATCH_THREADS;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint8_t *out_occ = nullptr;
+    double *out_f2 = nullptr;
+    ~hea_batch()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (void *p : buffers) cudaFree(p);
+        for (DeviceTables *t : tables) delete t;
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+struct BatchLevels {
+    unsigned long long total[kBatchLevels], base[kBatchLevels];
+};
+
+__global__ void batch_reset_kernel(BatchCtl *ctl, BatchJob *jobs, unsigned long long njobs, BatchLevels lv,
+                                   unsigned long long limit_ns)
+{
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < njobs;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        jobs[i].ready = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int l = 0; l < kBatchLevels; ++l) {
+            ctl->q[l].head = 0;
+            ctl->q[l].tail = 0;
+            ctl->q[l].total = lv.total[l];
+            ctl->q[l].base = lv.base[l];
+        }
+        for (int i = 0; i < 4; ++i) ctl->stats[i] = 0;
+        ctl->error = 0;
+        ctl->wait_limit_ns = limit_ns;
+    }
+}
+
+template <class X>
+int batch_alloc(hea_batch *b, X **p, size_t bytes)
+{
+    void *q = nullptr;
+    if (cudaMalloc(&q, bytes) != cudaSuccess) return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes", bytes);
+    b->buffers.push_back(q);
+    *p = static_cast<X *>(q);
+    return HEA_OK;
+}
+
+int batch_layout(const SearchConst &c, int S)
+{
+    if (S == 3 && c.chunks[0] == 2 && c.chunks[1] == 2 && c.chunks[2] == 3) return kLayBcc;
+    if (S == 3 && c.chunks[0] == 3 && c.chunks[1] == 2 && c.chunks[2] == 6) return kLayFccTrue;
+    return S == 1 ? kLayRt1 : (S == 2 ? kLayRt2 : kLayRt3);
+}
+
+}  // namespace
+
+extern "C" {
+
+int hea_batch_create(const hea_problem *problems, const hea_params *params, int32_t count, hea_batch **out)
+{
+    if (!out) return fail(HEA_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!problems || !params || count < 1) return fail(HEA_ERR_INVALID, "need at least one structure");
+    hea_batch *b = new (std::nothrow) hea_batch();
+    if (!b) return fail(HEA_ERR_NOMEM, "out of host memory");
+    b->count = count;
+    int rc = HEA_OK;
+    const int nwarps = b->block / 32;
+    for (int i = 0; i < count && rc == HEA_OK; ++i) {
+        rc = validate_params(&params[i]);
+        if (rc != HEA_OK) break;
+        DeviceTables *t = new (std::nothrow) DeviceTables();
+        if (!t) {
+            rc = fail(HEA_ERR_NOMEM, "out of host memory");
+            break;
+        }
+        b->tables.push_back(t);
+        rc = build_tables(&problems[i], params[i].seed, *t);
+        if (rc != HEA_OK) {
+            std::string m = g_error;
+            rc = fail(rc, "structure %d: %s", i, m.c_str());
+            break;
+        }
+        const int P = params[i].num_solutions, slots = 2 * P;
+        BatchStruct d{};
+        d.c = t->c;
+        d.nbor = t->nbor;
+        d.P = P;
+        d.Q = params[i].parallel_task;
+        d.D = params[i].converge_depth;
+        d.I = params[i].total_iter;
+        d.max_rounds = params[i].max_rounds > 0 ? params[i].max_rounds : (int64_t)1 << 31;
+        d.T = t->T;
+        d.layout = batch_layout(t->c, t->S);
+        if ((rc = batch_alloc(b, &d.occ, (size_t)slots * t->c.occ_stride)) != HEA_OK) break;
+        if ((rc = batch_alloc(b, &d.cnt, (size_t)slots * t->ncount * sizeof(int32_t))) != HEA_OK) break;
+        if ((rc = batch_alloc(b, &d.f2, (size_t)slots * sizeof(double))) != HEA_OK) break;
+        if ((rc = batch_alloc(b, &d.order, (size_t)slots * sizeof(int32_t))) != HEA_OK) break;
+        if ((rc = batch_alloc(b, &d.scratch, (size_t)slots * sizeof(int32_t))) != HEA_OK) break;
+        if (cudaMemset(d.occ, 0, (size_t)slots * t->c.occ_stride) != cudaSuccess) {
+            rc = fail(HEA_ERR_CUDA, "cudaMemset failed");
+            break;
+        }
+        b->h_structs.push_back(d);
+        b->total_jobs += d.I > 0 ? (unsigned long long)P * (2 * d.I + 1) : (unsigned long long)P;
+        const size_t sm = mc_smem(t->c.occ_stride, (int)t->ncount, nwarps);
+        if (sm > b->smem) b->smem = sm;
+    }
+    // priority levels: structures ranked by work, largest first
+    BatchLevels lv{};
+    if (rc == HEA_OK) {
+        std::vector<int> rank(count);
+        for (int i = 0; i < count; ++i) rank[i] = i;
+        auto work = [&](int i) {
+            const BatchStruct &d = b->h_structs[i];
+            return (double)d.c.num_sites * d.P * (2.0 * d.I + 1.0);
+        };
+        std::stable_sort(rank.begin(), rank.end(), [&](int x, int y) { return work(x) > work(y); });
+        for (int r = 0; r < count; ++r) {
+            BatchStruct &d = b->h_structs[rank[r]];
+            d.level = (int)((long long)r * kBatchLevels / count);
+            lv.total[d.level] += d.I > 0 ? (unsigned long long)d.P * (2 * d.I + 1) : (unsigned long long)d.P;
+        }
+        for (int l = 1; l < kBatchLevels; ++l) lv.base[l] = lv.base[l - 1] + lv.total[l - 1];
+    }
+    size_t max_out = 0;
+    for (int i = 0; rc == HEA_OK && i < count; ++i)
+        max_out = std::max(max_out, (size_t)b->h_structs[i].P * b->h_structs[i].c.num_sites);
+    if (rc == HEA_OK) rc = batch_alloc(b, &b->d_structs, sizeof(BatchStruct) * count);
+    if (rc == HEA_OK) rc = batch_alloc(b, &b->d_states, sizeof(BatchState) * count);
+    if (rc == HEA_OK) rc = batch_alloc(b, &b->d_jobs, sizeof(BatchJob) * b->total_jobs);
+    if (rc == HEA_OK) rc = batch_alloc(b, &b->d_ctl, sizeof(BatchCtl));
+    if (rc == HEA_OK) rc = batch_alloc(b, &b->d_finish, sizeof(unsigned long long) * count);
+    if (rc == HEA_OK) rc = batch_alloc(b, &b->out_occ, max_out);
+    if (rc == HEA_OK) rc = batch_alloc(b, &b->out_f2, sizeof(double) * 65536);
+    if (rc == HEA_OK) {
+        cudaFuncAttributes a;
+        if (cudaFuncGetAttributes(&a, batch_kernel) != cudaSuccess)
+            rc = fail(HEA_ERR_CUDA, "cannot query the batch kernel");
+        else if (b->smem + a.sharedSizeBytes > (size_t)smem_limit())
+            rc = fail(HEA_ERR_UNSUPPORTED, "the largest structure needs %zu bytes of shared memory, above %d", b->smem,
+                      smem_limit() - (int)a.sharedSizeBytes);
+    }
+    if (rc == HEA_OK) {
+        cudaError_t e = allow_max_smem(batch_kernel);
+        int per_sm = 0, sms = 0, dev = 0;
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, b->block, b->smem);
+        if (e == cudaSuccess) e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) rc = fail(HEA_ERR_CUDA, "batch kernel set-up failed: %s", cudaGetErrorString(e));
+        else if (per_sm < 1) rc = fail(HEA_ERR_UNSUPPORTED, "batch kernel does not fit on an SM");
+        b->grid = per_sm * sms;
+    }
+    if (rc == HEA_OK) {
+        cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
+        if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b->d_structs, b->h_structs.data(), sizeof(BatchStruct) * count, cudaMemcpyHostToDevice);
+        // the run as one CUDA graph: reset the queue, seed phase 0, persistent kernel
+        if (e == cudaSuccess) e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            batch_reset_kernel<<<64, 256, 0, b->stream>>>(b->d_ctl, b->d_jobs, b->total_jobs, lv, 60ull * 1000000000ull);
+            batch_seed_kernel<<<count, 256, 0, b->stream>>>(b->d_structs, b->d_states, b->d_jobs, b->d_ctl);
+            batch_kernel<<<b->grid, b->block, b->smem, b->stream>>>(b->d_structs, b->d_states, b->d_jobs, b->d_ctl,
+                                                                    b->d_finish);
+            cudaError_t e2 = cudaStreamEndCapture(b->stream, &b->graph);
+            e = e2;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+        if (e != cudaSuccess) rc = fail(HEA_ERR_CUDA, "batch graph set-up failed: %s", cudaGetErrorString(e));
+    }
+    if (rc != HEA_OK) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return HEA_OK;
+}
+
+int hea_batch_run(hea_batch *b, const uint64_t *seeds, hea_stats *stats)
+{
+    if (!b) return fail(HEA_ERR_INVALID, "batch is NULL");
+    if (seeds) {
+        for (int i = 0; i < b->count; ++i) {
+            b->h_structs[i].c.key0 = (uint32_t)seeds[i];
+            b->h_structs[i].c.key1 = (uint32_t)(seeds[i] >> 32);
+        }
+        HEA_CUDA(cudaMemcpyAsync(b->d_structs, b->h_structs.data(), sizeof(BatchStruct) * b->count,
+                                 cudaMemcpyHostToDevice, b->stream));
+    }
+    HEA_CUDA(cudaEventRecord(b->ev0, b->stream));
+    HEA_CUDA(cudaGraphLaunch(b->exec, b->stream));
+    HEA_CUDA(cudaEventRecord(b->ev1, b->stream));
+    HEA_CUDA(cudaStreamSynchronize(b->stream));
+    BatchCtl ctl;
+    HEA_CUDA(cudaMemcpy(&ctl, b->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+    if (ctl.error)
+        return fail(HEA_ERR_CUDA, "batched search stopped: a wait for queued work exceeded its time limit");
+    if (ctl.stats[3] != (unsigned long long)b->count)
+        return fail(HEA_ERR_CUDA, "batched search finished %llu of %d structures", ctl.stats[3], b->count);
+    if (stats) {
+        float ms = 0;
+        HEA_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+        stats->rounds = (int64_t)ctl.stats[0];
+        stats->evals = (int64_t)ctl.stats[1];
+        stats->accepts = (int64_t)ctl.stats[2];
+        stats->gpu_ms = ms;
+        stats->mc_ms = ms;
+        stats->mc_launches = 1;
+    }
+    return HEA_OK;
+}
+
+int hea_batch_read(hea_batch *b, int32_t index, uint8_t *out_occ, double *out_fitness)
+{
+    if (!b || index < 0 || index >= b->count) return fail(HEA_ERR_INVALID, "no structure %d in the batch", index);
+    const BatchStruct &d = b->h_structs[index];
+    dim3 grid((d.c.num_sites + 255) / 256 < 64 ? (d.c.num_sites + 255) / 256 : 64, d.P);
+    gather_rows_kernel<<<grid, 256, 0, b->stream>>>(d.occ, d.order, d.P, d.c.occ_stride, d.c.num_sites, d.f2,
+                                                    b->out_occ, b->out_f2);
+    HEA_CUDA(cudaGetLastError());
+    if (out_occ)
+        HEA_CUDA(cudaMemcpyAsync(out_occ, b->out_occ, (size_t)d.P * d.c.num_sites, cudaMemcpyDeviceToHost, b->stream));
+    std::vector<double> f(d.P);
+    HEA_CUDA(cudaMemcpyAsync(f.data(), b->out_f2, d.P * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    HEA_CUDA(cudaStreamSynchronize(b->stream));
+    if (out_fitness)
+        for (int p = 0; p < d.P; ++p) out_fitness[p] = std::sqrt(f[p]);
+    return HEA_OK;
+}
+
+int hea_batch_finish_times(hea_batch *b, double *out_ms)
+{
+    if (!b || !out_ms) return fail(HEA_ERR_INVALID, "batch and out_ms must not be NULL");
+    std::vector<unsigned long long> ns(b->count);
+    HEA_CUDA(cudaMemcpy(ns.data(), b->d_finish, sizeof(unsigned long long) * b->count, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < b->count; ++i) out_ms[i] = ns[i] * 1e-6;
+    return HEA_OK;
+}
+
+void hea_batch_destroy(hea_batch *b) { delete b; }
+
+}  // extern "C"

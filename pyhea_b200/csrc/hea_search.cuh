@@ -208,7 +208,10 @@ __device__ __forceinline__ double shell_error(const SearchConst &c, const int32_
 
 // Score one proposal: f2 of the counts after swapping s1 (species a) and s2 (b).
 // Returns the per-shell histograms so the accept step can apply the change.
-template <int T, class L>
+// kAhead (fixed layouts): issue the loads of every shell of both rows before
+// the first use -- one L2 round trip per proposal instead of one per shell, at
+// the cost of holding the whole rows in registers.
+template <int T, class L, bool kAhead = false>
 __device__ __forceinline__ double score_swap(const SearchConst &c, const int4 *__restrict__ nbor, const uint8_t *occ5,
                                              const int32_t *cnt, uint32_t s1, uint32_t s2, int a, int b,
                                              uint32_t (&h1)[L::S], uint32_t (&h2)[L::S], int (&m)[L::S])
@@ -216,10 +219,34 @@ __device__ __forceinline__ double score_swap(const SearchConst &c, const int4 *_
     const int row4 = L::kRuntime ? c.row4 : L::kRow4;
     const int4 *r1 = nbor + (size_t)s1 * row4;
     const int4 *r2 = nbor + (size_t)s2 * row4;
+    if constexpr (kAhead && !L::kRuntime) {
+        constexpr int kRow = L::kRow4 > 0 ? L::kRow4 : 1;
+        int4 x[kRow], y[kRow];
+#pragma unroll
+        for (int ch = 0; ch < kRow; ++ch) {
+            x[ch] = __ldg(r1 + ch);
+            y[ch] = __ldg(r2 + ch);
+        }
+#pragma unroll
+        for (int k = 0; k < L::S; ++k) {
+            h1[k] = 0;
+            h2[k] = 0;
+            m[k] = 0;
+#pragma unroll
+            for (int ch = 0; ch < kRow; ++ch)
+                if (ch >= L::off(k) && ch < L::off(k) + L::chunks(k)) {
+                    h1[k] += hist4(x[ch], occ5);
+                    h2[k] += hist4(y[ch], occ5);
+                    m[k] += count4(x[ch], s2);
+                }
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < L::S; ++k) shell_hist<L>(c, r1, r2, occ5, s2, k, h1[k], h2[k], m[k]);
+    }
     double f2 = 0.0;
 #pragma unroll
     for (int k = 0; k < L::S; ++k) {
-        shell_hist<L>(c, r1, r2, occ5, s2, k, h1[k], h2[k], m[k]);
         int u[T];
         delta_vector<T>(h1[k], h2[k], m[k], a, b, u);
         f2 = __fma_rn(c.w[k], shell_error<T>(c, cnt, k, u, a, b), f2);
@@ -327,10 +354,34 @@ __device__ void block_recount(const SearchConst &c, const int4 *__restrict__ nbo
 }
 
 // ---------------------------------------------------------------------------
-// New random occupancy (keyed Feistel permutation of the sorted layout) or a
-// recount of a stored one; writes occupancy, counts and f2 of the slot.
-// One CTA per slot; dynamic shared memory = occ_stride + 16 + 4*S*T*T bytes.
+// Random occupancy of population position `pos` of generation `generation`:
+// the sorted species layout read through a keyed Feistel permutation (cycle
+// walking).  Writes 5*species into occ5 and, when gocc != nullptr, species
+// into the slot's row in HBM.  Block-cooperative; no barrier inside.
 // ---------------------------------------------------------------------------
+template <int T>
+__device__ __forceinline__ void generate_occupancy(const SearchConst &c, uint32_t pos, uint32_t generation,
+                                                   uint8_t *occ5, uint8_t *gocc)
+{
+    uint32_t rk[kFeistelRounds];
+    const u32x4 w0 = philox4x32_10(u32x4{pos, generation, 0u, kInitStream}, c.key0, c.key1);
+    const u32x4 w1 = philox4x32_10(u32x4{pos, generation, 1u, kInitStream}, c.key0, c.key1);
+    rk[0] = w0.x; rk[1] = w0.y; rk[2] = w0.z; rk[3] = w0.w; rk[4] = w1.x; rk[5] = w1.y;
+    const int n = c.num_sites;
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+        uint32_t y = feistel((uint32_t)s, c.feistel_h, rk);
+        while (y >= (uint32_t)n) y = feistel(y, c.feistel_h, rk);
+        int t = 0;
+#pragma unroll
+        for (int i = 1; i < T; ++i) t += (int)(y >= (uint32_t)c.prefix[i]);
+        occ5[s] = (uint8_t)(5 * t);
+        if (gocc) gocc[s] = (uint8_t)t;
+    }
+}
+
+// New random occupancy or a recount of a stored one; writes occupancy, counts
+// and f2 of the slot.  One CTA per slot; dynamic shared memory = occ_stride +
+// 16 + 4*S*T*T bytes.
 template <int T, int S>
 __global__ void __launch_bounds__(512, 1) generate_kernel(const SearchConst c, const GenArgs g)
 {
@@ -341,19 +392,7 @@ __global__ void __launch_bounds__(512, 1) generate_kernel(const SearchConst c, c
     uint8_t *gocc = g.occ + (size_t)slot * c.occ_stride;
     const int n = c.num_sites;
     if (g.generate) {
-        uint32_t rk[kFeistelRounds];
-        const u32x4 w0 = philox4x32_10(u32x4{blockIdx.x, g.generation, 0u, kInitStream}, c.key0, c.key1);
-        const u32x4 w1 = philox4x32_10(u32x4{blockIdx.x, g.generation, 1u, kInitStream}, c.key0, c.key1);
-        rk[0] = w0.x; rk[1] = w0.y; rk[2] = w0.z; rk[3] = w0.w; rk[4] = w1.x; rk[5] = w1.y;
-        for (int s = threadIdx.x; s < n; s += blockDim.x) {
-            uint32_t y = feistel((uint32_t)s, c.feistel_h, rk);
-            while (y >= (uint32_t)n) y = feistel(y, c.feistel_h, rk);
-            int t = 0;
-#pragma unroll
-            for (int i = 1; i < T; ++i) t += (int)(y >= (uint32_t)c.prefix[i]);
-            occ5[s] = (uint8_t)(5 * t);
-            gocc[s] = (uint8_t)t;
-        }
+        generate_occupancy<T>(c, blockIdx.x, g.generation, occ5, gocc);
     } else {
         for (int s = threadIdx.x; s < n; s += blockDim.x) occ5[s] = (uint8_t)(5 * gocc[s]);
     }
@@ -378,7 +417,7 @@ __global__ void __launch_bounds__(512, 1) generate_kernel(const SearchConst c, c
 // shared occupancy (all threads write the same two bytes) and applies the count
 // change to its own copy of the counts, so no second barrier is needed before
 // the next round reads them.
-// Dynamic shared memory: occ_stride + 16 + nwarps * 4 * ncount_pad + 2 * 32 * sizeof(SwapRecord).
+// Shared memory: occ_stride + 16 + nwarps * (4 * ncount_pad + 2 * sizeof(SwapRecord)).
 // ---------------------------------------------------------------------------
 struct SwapRecord {
     double f2;
@@ -393,46 +432,32 @@ static_assert(sizeof(SwapRecord) == 56, "SwapRecord layout");
 
 __host__ __device__ constexpr int mc_ncount_pad(int ncount) { return (ncount + 3) & ~3; }
 
-#ifndef HEA_MC_MIN_BLOCKS
-#define HEA_MC_MIN_BLOCKS 2  // resident 512-thread blocks per SM the register budget aims for
-#endif
-template <int T, class L>
-__global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const SearchConst c, const McArgs g)
+struct McTrace {
+    AcceptRecord *records;  // trace_cap records for this search, or nullptr
+    int32_t *counts;        // trace_cap count snapshots, or nullptr
+    int64_t cap;
+};
+
+struct McTally {
+    double f2;
+    int64_t rounds, accepts, evals;
+};
+
+// Rounds of the local search on the staged state (occ5, the per-warp count
+// copies in cnt_all).  Every thread returns the same f2/rounds/accepts; evals
+// is this thread's count.  No barrier at entry; one per round.
+template <int T, class L, bool kAhead = false>
+__device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *__restrict__ nbor, uint8_t *occ5,
+                                             int32_t *cnt_all, SwapRecord *rec, uint32_t stream, double cur,
+                                             int tasks, int depth, int64_t max_rounds, McTrace tr)
 {
     constexpr int S = L::S, NC = S * T * T, NCP = mc_ncount_pad(NC);
-    extern __shared__ __align__(16) uint8_t smem[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    uint8_t *occ5 = smem;
-    int32_t *cnt_all = reinterpret_cast<int32_t *>(smem + c.occ_stride + 16);
     int32_t *cnt = cnt_all + warp * NCP;  // this warp's copy of the counts
-    SwapRecord *rec = reinterpret_cast<SwapRecord *>(cnt_all + nwarps * NCP);  // [2][32]
-
-    const int slot = g.order[blockIdx.x];
-    const uint32_t stream = (g.mc_call << 16) | (uint32_t)blockIdx.x;
-    uint8_t *gocc = g.occ + (size_t)slot * c.occ_stride;
-    int32_t *gcnt = g.cnt + (size_t)slot * NC;
-    const int n = c.num_sites;
-
-    {  // stage the slot: occupancy as 5*species (16-byte vectors), counts per warp
-        const uint4 *src = reinterpret_cast<const uint4 *>(gocc);
-        uint4 *dst = reinterpret_cast<uint4 *>(occ5);
-        for (int v = tid; v < c.occ_stride / 16; v += blockDim.x) {
-            uint4 x = src[v];
-            // bytes are species < 8: 5*t per byte without carries
-            x.x = x.x * 5u; x.y = x.y * 5u; x.z = x.z * 5u; x.w = x.w * 5u;
-            dst[v] = x;
-        }
-        for (int x = lane; x < NC; x += 32) cnt[x] = gcnt[x];
-    }
-    __syncthreads();
-    if (tid == 0) occ5[n] = 0;  // sentinel (occ_stride may end exactly at n)
-    __syncthreads();
-
-    double cur = g.f2[slot];
     int miss = 0;
     int64_t round = 0, accepts = 0, evals = 0;
-    while (miss < g.depth && round < g.max_rounds) {
-        SwapRecord *rr = rec + (round & 1) * 32;
+    while (miss < depth && round < max_rounds) {
+        SwapRecord *rr = rec + (round & 1) * nwarps;
         SwapRecord &mine = rr[warp];  // this warp's best proposal of the round
         if (lane == 0) {
             mine.f2 = inf_d();
@@ -440,10 +465,10 @@ __global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const Search
         }
         __syncwarp();
         // passes of blockDim tasks; lane q of a pass scores task q (warp-uniform trip count)
-        for (int q0 = warp * 32; q0 < g.tasks; q0 += blockDim.x) {
+        for (int q0 = warp * 32; q0 < tasks; q0 += blockDim.x) {
             const int q = q0 + lane;
             uint32_t s1 = 0, s2 = 0;
-            const bool ok = q < g.tasks && draw_pair(c, stream, (uint32_t)round, (uint32_t)q, occ5, s1, s2);
+            const bool ok = q < tasks && draw_pair(c, stream, (uint32_t)round, (uint32_t)q, occ5, s1, s2);
             __syncwarp();  // lanes that needed more draws rejoin before scoring
             double f = inf_d();
             uint32_t h1[S], h2[S];
@@ -452,7 +477,7 @@ __global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const Search
                 ++evals;
                 a = occ5[s1] / 5;
                 b = occ5[s2] / 5;
-                f = score_swap<T, L>(c, g.nbor, occ5, cnt, s1, s2, a, b, h1, h2, m);
+                f = score_swap<T, L, kAhead>(c, nbor, occ5, cnt, s1, s2, a, b, h1, h2, m);
             }
             double wf = f;
             int wq = ok ? q : 0x7FFFFFFF;
@@ -509,7 +534,7 @@ __global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const Search
                 cnt[x] += ((i == a) - (i == b)) * uj + ((j == a) - (j == b)) * ui;
             }
             __syncwarp();
-            if (g.trace && warp == 0 && accepts < g.trace_cap) {
+            if (tr.records && warp == 0 && accepts < tr.cap) {
                 if (lane == 0) {
                     AcceptRecord r;
                     r.round = (uint32_t)round;
@@ -517,10 +542,10 @@ __global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const Search
                     r.s1 = w.s1;
                     r.s2 = w.s2;
                     r.f2 = xf;
-                    g.trace[(size_t)blockIdx.x * g.trace_cap + accepts] = r;
+                    tr.records[accepts] = r;
                 }
-                if (g.trace_counts) {
-                    int32_t *dst = g.trace_counts + ((size_t)blockIdx.x * g.trace_cap + accepts) * NC;
+                if (tr.counts) {
+                    int32_t *dst = tr.counts + accepts * NC;
                     for (int x = lane; x < NC; x += 32) dst[x] = cnt[x];
                 }
             }
@@ -533,41 +558,103 @@ __global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const Search
         ++round;
     }
     __syncthreads();
+    return McTally{cur, round, accepts, evals};
+}
 
-    // write the slot back
-    {
-        const uint4 *src = reinterpret_cast<const uint4 *>(occ5);
-        uint4 *dst = reinterpret_cast<uint4 *>(gocc);
-        for (int v = tid; v < c.occ_stride / 16; v += blockDim.x) {
-            uint4 x = src[v];
-            // every byte holds 5*t with t < 8: t = (5t * 205) >> 10 per byte
-            uint32_t o[4] = {x.x, x.y, x.z, x.w};
-#pragma unroll
-            for (int w = 0; w < 4; ++w) {
-                uint32_t r = 0;
-#pragma unroll
-                for (int by = 0; by < 4; ++by) {
-                    const uint32_t b5 = (o[w] >> (8 * by)) & 0xFFu;
-                    r |= ((b5 * 205u) >> 10) << (8 * by);
-                }
-                o[w] = r;
-            }
-            dst[v] = make_uint4(o[0], o[1], o[2], o[3]);
-        }
-        if (warp == 0)
-            for (int x = lane; x < NC; x += 32) gcnt[x] = cnt[x];
+// Slot row (species bytes) -> 5*species in shared memory (16-byte vectors).
+// kFromL2: load through L2 only (rows written earlier by other CTAs of the
+// same launch may sit stale in this SM's L1).
+template <bool kFromL2 = false>
+__device__ __forceinline__ void stage_occupancy(const SearchConst &c, const uint8_t *gocc, uint8_t *occ5)
+{
+    const uint4 *src = reinterpret_cast<const uint4 *>(gocc);
+    uint4 *dst = reinterpret_cast<uint4 *>(occ5);
+    for (int v = threadIdx.x; v < c.occ_stride / 16; v += blockDim.x) {
+        uint4 x = kFromL2 ? __ldcg(src + v) : src[v];
+        // bytes are species < 8: 5*t per byte without carries
+        x.x = x.x * 5u; x.y = x.y * 5u; x.z = x.z * 5u; x.w = x.w * 5u;
+        dst[v] = x;
     }
-    // evals per thread -> block total
-    unsigned long long ev = (unsigned long long)evals;
+}
+
+// 5*species in shared memory -> slot row (species bytes).
+__device__ __forceinline__ void unstage_occupancy(const SearchConst &c, const uint8_t *occ5, uint8_t *gocc)
+{
+    const uint4 *src = reinterpret_cast<const uint4 *>(occ5);
+    uint4 *dst = reinterpret_cast<uint4 *>(gocc);
+    for (int v = threadIdx.x; v < c.occ_stride / 16; v += blockDim.x) {
+        uint4 x = src[v];
+        // every byte holds 5*t with t < 8: t = (5t * 205) >> 10 per byte
+        uint32_t o[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            uint32_t r = 0;
+#pragma unroll
+            for (int by = 0; by < 4; ++by) {
+                const uint32_t b5 = (o[w] >> (8 * by)) & 0xFFu;
+                r |= ((b5 * 205u) >> 10) << (8 * by);
+            }
+            o[w] = r;
+        }
+        dst[v] = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+}
+
+// Sum of per-thread evaluation counts of the block, added to stats[1];
+// rounds and accepts (uniform) to stats[0] and stats[2] by thread 0.
+__device__ __forceinline__ void add_tally(const McTally &t, unsigned long long *stats)
+{
+    unsigned long long ev = (unsigned long long)t.evals;
 #pragma unroll
     for (int o = 16; o; o >>= 1) ev += __shfl_xor_sync(0xFFFFFFFFu, ev, o);
-    if (lane == 0 && ev) atomicAdd(&g.stats[1], ev);
+    if ((threadIdx.x & 31) == 0 && ev) atomicAdd(&stats[1], ev);
+    if (threadIdx.x == 0) {
+        atomicAdd(&stats[0], (unsigned long long)t.rounds);
+        atomicAdd(&stats[2], (unsigned long long)t.accepts);
+    }
+}
+
+#ifndef HEA_MC_MIN_BLOCKS
+#define HEA_MC_MIN_BLOCKS 2  // resident 512-thread blocks per SM the register budget aims for
+#endif
+template <int T, class L>
+__global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const SearchConst c, const McArgs g)
+{
+    constexpr int S = L::S, NC = S * T * T, NCP = mc_ncount_pad(NC);
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    uint8_t *occ5 = smem;
+    int32_t *cnt_all = reinterpret_cast<int32_t *>(smem + c.occ_stride + 16);
+    SwapRecord *rec = reinterpret_cast<SwapRecord *>(cnt_all + nwarps * NCP);  // [2][nwarps]
+
+    const int slot = g.order[blockIdx.x];
+    const uint32_t stream = (g.mc_call << 16) | (uint32_t)blockIdx.x;
+    uint8_t *gocc = g.occ + (size_t)slot * c.occ_stride;
+    int32_t *gcnt = g.cnt + (size_t)slot * NC;
+
+    stage_occupancy(c, gocc, occ5);
+    for (int x = lane; x < NC; x += 32) cnt_all[warp * NCP + x] = gcnt[x];
+    __syncthreads();
+    if (tid == 0) occ5[c.num_sites] = 0;  // sentinel (occ_stride may end exactly at n)
+    __syncthreads();
+
+    McTrace tr{nullptr, nullptr, 0};
+    if (g.trace) {
+        tr.records = g.trace + (size_t)blockIdx.x * g.trace_cap;
+        tr.counts = g.trace_counts ? g.trace_counts + (size_t)blockIdx.x * g.trace_cap * NC : nullptr;
+        tr.cap = g.trace_cap;
+    }
+    const McTally t = mc_rounds<T, L>(c, g.nbor, occ5, cnt_all, rec, stream, g.f2[slot], g.tasks, g.depth,
+                                      g.max_rounds, tr);
+
+    unstage_occupancy(c, occ5, gocc);
+    if (warp == 0)
+        for (int x = lane; x < NC; x += 32) gcnt[x] = cnt_all[x];
+    add_tally(t, g.stats);
     if (tid == 0) {
-        g.f2[slot] = cur;
-        atomicAdd(&g.stats[0], (unsigned long long)round);
-        atomicAdd(&g.stats[2], (unsigned long long)accepts);
-        if (g.trace_len) g.trace_len[blockIdx.x] = accepts;
-        if (g.rounds_out) g.rounds_out[blockIdx.x] = round;
+        g.f2[slot] = t.f2;
+        if (g.trace_len) g.trace_len[blockIdx.x] = t.accepts;
+        if (g.rounds_out) g.rounds_out[blockIdx.x] = t.rounds;
     }
 }
 

@@ -208,3 +208,20 @@ def test_full_size_plain_gpu_properties():
     assert stats["evals"] > 0 and stats["accepts"] > 0
     init = hb.generate(gp, 11, 0, st.P)[2]
     assert fit[0] ** 2 < init.min()
+
+
+def test_plans_of_different_sizes_coexist():
+    """Kernels are shared by all plans: creating a plan for a small structure
+    must not shrink the shared-memory allowance of a larger plan made before."""
+    big = W.small_case(lattice=L.FCC, cell=14, species=(2744,) * 4, shell_set=L.SHELLS_FCC_TRUE3)
+    small = W.small_case(lattice=L.FCC, cell=3, species=(27,) * 4, shell_set=L.SHELLS_FCC_TRUE3)
+    pb_big, pb_small = big.problem(), small.problem()
+    plan_big = hb.Plan(pb_big, 2, 1, 64, 2)
+    plan_small = hb.Plan(pb_small, 2, 1, 64, 2)
+    hb.recount_noalloc(pb_small, hb.generate(pb_small, 1, 0, 1)[0])
+    plan_big.run(3)
+    plan_small.run(3)
+    occ, fit = plan_big.read()
+    np.testing.assert_array_equal(np.sqrt(hb.recount(pb_big, occ)[1]), fit)
+    plan_big.close()
+    plan_small.close()
