@@ -32,6 +32,8 @@ extern "C" {
 
 #define HEA_FLAG_LOG_ITERS 1    /* print the per-iteration best fitness line, as accelerate.cu:1208-1212 does */
 #define HEA_FLAG_TIME_KERNELS 2 /* time every local-search launch with CUDA events (hea_stats.mc_ms)        */
+#define HEA_FLAG_HBM_OCCUPANCY 4 /* keep occupancies in HBM and search each solution with a thread-block
+                                    cluster -- the path structures too large for shared memory always take */
 
 /* One structure to search.  Mirrors the arguments nbor, element, weight and
  * target_sro of run_local_parallel_hcs_cuda (bind.cpp:55-58). */

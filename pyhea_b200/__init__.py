@@ -29,6 +29,7 @@ _i32, _i64, _u32, _u64, _f64, _u8 = (ctypes.c_int32, ctypes.c_int64, ctypes.c_ui
 HEA_OK, HEA_ERR_INVALID, HEA_ERR_UNSUPPORTED, HEA_ERR_CUDA, HEA_ERR_NOMEM = 0, 1, 2, 3, 4
 HEA_FLAG_LOG_ITERS = 1
 HEA_FLAG_TIME_KERNELS = 2
+HEA_FLAG_HBM_OCCUPANCY = 4
 FCC, BCC = 0, 1
 SHELLS_REFERENCE, SHELLS_FCC_TRUE3 = 0, 1
 
@@ -144,14 +145,15 @@ def _params(num_solutions, total_iter, parallel_task, converge_depth, seed, max_
 
 
 def search(problem, num_solutions, total_iter, parallel_task, converge_depth, seed=0, max_rounds=0, log=False,
-           out_occ=None, out_fitness=None, time_kernels=False):
+           out_occ=None, out_fitness=None, time_kernels=False, hbm_occupancy=False):
     """The whole search with host buffers (hea_run_local_parallel_hcs).
     Returns (occ [P][N] uint8, fitness [P] float64, stats dict)."""
     P, N = int(num_solutions), problem.num_sites
     occ = out_occ if out_occ is not None else np.empty((P, N), dtype=np.uint8)
     fit = out_fitness if out_fitness is not None else np.empty(P, dtype=np.float64)
     st = Stats()
-    flags = (HEA_FLAG_LOG_ITERS if log else 0) | (HEA_FLAG_TIME_KERNELS if time_kernels else 0)
+    flags = ((HEA_FLAG_LOG_ITERS if log else 0) | (HEA_FLAG_TIME_KERNELS if time_kernels else 0) |
+             (HEA_FLAG_HBM_OCCUPANCY if hbm_occupancy else 0))
     prm = _params(P, total_iter, parallel_task, converge_depth, seed, max_rounds, flags)
     _check(lib.hea_run_local_parallel_hcs(ctypes.byref(problem._c), ctypes.byref(prm), _ptr(occ, _u8),
                                           _ptr(fit, _f64), ctypes.byref(st)))
@@ -162,12 +164,12 @@ class Plan:
     """Device-resident search (hea_plan_*): tables uploaded once, run many times."""
 
     def __init__(self, problem, num_solutions, total_iter, parallel_task, converge_depth, seed=0, max_rounds=0,
-                 time_kernels=False):
+                 time_kernels=False, hbm_occupancy=False):
         self.problem = problem
         self.P = int(num_solutions)
         self._h = ctypes.c_void_p()
-        prm = _params(num_solutions, total_iter, parallel_task, converge_depth, seed, max_rounds,
-                      HEA_FLAG_TIME_KERNELS if time_kernels else 0)
+        flags = (HEA_FLAG_TIME_KERNELS if time_kernels else 0) | (HEA_FLAG_HBM_OCCUPANCY if hbm_occupancy else 0)
+        prm = _params(num_solutions, total_iter, parallel_task, converge_depth, seed, max_rounds, flags)
         _check(lib.hea_plan_create(ctypes.byref(problem._c), ctypes.byref(prm), ctypes.byref(self._h)))
 
     def run(self, seed):

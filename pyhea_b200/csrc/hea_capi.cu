@@ -17,6 +17,7 @@
 
 #include "hea_cuda.h"
 #include "hea_search.cuh"
+#include "hea_large.cuh"
 
 using namespace hea;
 
@@ -74,6 +75,51 @@ McFn pick_mc_t(int c0, int c1, int c2, int S)
     if (S == 1) return mc_kernel<T, RuntimeShells<1>>;
     if (S == 2) return mc_kernel<T, RuntimeShells<2>>;
     return mc_kernel<T, RuntimeShells<3>>;
+}
+
+// The same choice for the HBM-occupancy (cluster) search.
+template <int T>
+McFn pick_mc_large_t(int c0, int c1, int c2, int S)
+{
+    if (c0 == 2 && c1 == 2 && c2 == 3) return mc_large_kernel<T, Shells<2, 2, 3>>;
+    if (c0 == 3 && c1 == 2 && c2 == 3) return mc_large_kernel<T, Shells<3, 2, 3>>;
+    if (c0 == 3 && c1 == 2 && c2 == 6) return mc_large_kernel<T, Shells<3, 2, 6>>;
+    if (S == 1) return mc_large_kernel<T, RuntimeShells<1>>;
+    if (S == 2) return mc_large_kernel<T, RuntimeShells<2>>;
+    return mc_large_kernel<T, RuntimeShells<3>>;
+}
+
+McFn pick_mc_large(int T, int c0, int c1, int c2, int S)
+{
+    switch (T) {
+    case 2: return pick_mc_large_t<2>(c0, c1, c2, S);
+    case 3: return pick_mc_large_t<3>(c0, c1, c2, S);
+    case 4: return pick_mc_large_t<4>(c0, c1, c2, S);
+    case 5: return pick_mc_large_t<5>(c0, c1, c2, S);
+    default: return pick_mc_large_t<6>(c0, c1, c2, S);
+    }
+}
+
+using LGenFn = void (*)(const SearchConst, uint8_t *, const int32_t *, uint32_t);
+using LRecFn = void (*)(const SearchConst, const int4 *, const uint8_t *, const int32_t *, int32_t *);
+using LFitFn = void (*)(const SearchConst, const int32_t *, int, const int32_t *, double *);
+const LGenFn kLGen[kMaxTypes + 1] = {nullptr, nullptr, large_generate_kernel<2>, large_generate_kernel<3>,
+                                     large_generate_kernel<4>, large_generate_kernel<5>, large_generate_kernel<6>};
+#define HEA_LREC_ROW(T) {nullptr, large_recount_kernel<T, 1>, large_recount_kernel<T, 2>, large_recount_kernel<T, 3>}
+const LRecFn kLRec[kMaxTypes + 1][kMaxShells + 1] = {
+    {nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}, HEA_LREC_ROW(2), HEA_LREC_ROW(3),
+    HEA_LREC_ROW(4), HEA_LREC_ROW(5), HEA_LREC_ROW(6)};
+#define HEA_LFIT_ROW(T) {nullptr, large_fitness_kernel<T, 1>, large_fitness_kernel<T, 2>, large_fitness_kernel<T, 3>}
+const LFitFn kLFit[kMaxTypes + 1][kMaxShells + 1] = {
+    {nullptr, nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr, nullptr}, HEA_LFIT_ROW(2), HEA_LFIT_ROW(3),
+    HEA_LFIT_ROW(4), HEA_LFIT_ROW(5), HEA_LFIT_ROW(6)};
+
+__global__ void zero_counts_kernel(const int32_t *order, int count, int32_t *cnt, int ncount)
+{
+    const int p = blockIdx.y;
+    if (p >= count) return;
+    int32_t *g = cnt + (size_t)order[p] * ncount;
+    for (int x = threadIdx.x; x < ncount; x += blockDim.x) g[x] = 0;
 }
 
 McFn pick_mc(int T, int c0, int c1, int c2, int S)
@@ -270,6 +316,10 @@ struct DeviceTables {
     GenFn gen = nullptr;
     McFn mc = nullptr;
     int mc_block = 0;
+    bool large = false;  // occupancy in HBM, one cluster per solution (hea_large.cuh)
+    LGenFn lgen = nullptr;
+    LRecFn lrec = nullptr;
+    LFitFn lfit = nullptr;
     ~DeviceTables()
     {
         if (nbor) cudaFree(nbor);
@@ -355,7 +405,7 @@ cudaError_t allow_max_smem(F *func)
     return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_limit() - (int)a.sharedSizeBytes);
 }
 
-int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt)
+int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t flags = 0)
 {
     HEA_TRY(validate_problem(pb));
     const int T = pb->num_types, S = pb->num_shells, N = pb->num_sites;
@@ -389,7 +439,7 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt)
     c.num_sites = N;
     c.num_types = T;
     c.num_shells = S;
-    c.occ_stride = (N + 15) & ~15;
+    c.occ_stride = (N + 1 + 15) & ~15;  // room for the sentinel byte N in HBM rows too
     c.feistel_h = feistel_half_bits((uint32_t)N);
     c.reject_below = (uint32_t)(0u - (uint32_t)N) % (uint32_t)N;
     c.key0 = (uint32_t)seed;
@@ -410,15 +460,20 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt)
     const size_t cnt_bytes = 4 * (size_t)((dt.ncount + 3) & ~3);
     dt.smem_gen = (size_t)c.occ_stride + 16 + cnt_bytes;
     dt.smem_mc = mc_smem(c.occ_stride, (int)dt.ncount, 16);  // the largest block (512 threads)
-    if (dt.smem_mc > (size_t)smem_limit())
-        return fail(HEA_ERR_UNSUPPORTED,
-                    "%d sites need %zu bytes of shared memory per solution, above the %d-byte limit of the "
-                    "shared-memory search path",
-                    N, dt.smem_mc, smem_limit());
-    dt.gen = kGen[T][S];
-    dt.mc = pick_mc(T, c.chunks[0], S > 1 ? c.chunks[1] : 0, S > 2 ? c.chunks[2] : 0, S);
-    HEA_CUDA(allow_max_smem(dt.gen));
-    HEA_CUDA(allow_max_smem(dt.mc));
+    if (dt.smem_mc > (size_t)smem_limit() || (flags & HEA_FLAG_HBM_OCCUPANCY)) {
+        // structures beyond shared memory: occupancy in HBM, cluster search
+        dt.large = true;
+        dt.mc = pick_mc_large(T, c.chunks[0], S > 1 ? c.chunks[1] : 0, S > 2 ? c.chunks[2] : 0, S);
+        dt.lgen = kLGen[T];
+        dt.lrec = kLRec[T][S];
+        dt.lfit = kLFit[T][S];
+        HEA_CUDA(allow_max_smem(dt.mc));
+    } else {
+        dt.gen = kGen[T][S];
+        dt.mc = pick_mc(T, c.chunks[0], S > 1 ? c.chunks[1] : 0, S > 2 ? c.chunks[2] : 0, S);
+        HEA_CUDA(allow_max_smem(dt.gen));
+        HEA_CUDA(allow_max_smem(dt.mc));
+    }
 
     // padded table on the device, checked
     const size_t raw_bytes = (size_t)N * raw_row * sizeof(int32_t);
@@ -504,6 +559,18 @@ int launch_generate(hea_plan *pl, const int32_t *order, int count, uint32_t gene
     a.order = order;
     a.generation = generation;
     a.generate = generate;
+    if (pl->dt.large) {
+        const SearchConst &c = pl->dt.c;
+        int chunks = (c.num_sites + 255) / 256;
+        const int cap = std::max(1, 2368 / count);
+        if (chunks > cap) chunks = cap;
+        zero_counts_kernel<<<dim3(1, count), 128, 0, st>>>(order, count, pl->cnt, (int)pl->dt.ncount);
+        if (generate) pl->dt.lgen<<<dim3(chunks, count), 256, 0, st>>>(c, pl->occ, order, generation);
+        pl->dt.lrec<<<dim3(chunks, count), 256, 0, st>>>(c, pl->dt.nbor, pl->occ, order, pl->cnt);
+        pl->dt.lfit<<<(count + 127) / 128, 128, 0, st>>>(c, order, count, pl->cnt, pl->f2);
+        HEA_CUDA(cudaGetLastError());
+        return HEA_OK;
+    }
     pl->dt.gen<<<count, 512, pl->dt.smem_gen, st>>>(pl->dt.c, a);
     HEA_CUDA(cudaGetLastError());
     return HEA_OK;
@@ -525,8 +592,30 @@ int launch_mc(hea_plan *pl, const int32_t *order, int count, uint32_t mc_call, M
     a.stats = pl->stats;
     const bool timed = (pl->prm.flags & HEA_FLAG_TIME_KERNELS) && 2 * pl->mc_timed + 1 < (int)pl->mc_events.size();
     if (timed) HEA_CUDA(cudaEventRecord(pl->mc_events[2 * pl->mc_timed], st));
-    const int block = choose_block(a.tasks);
-    pl->dt.mc<<<count, block, mc_smem(pl->dt.c.occ_stride, (int)pl->dt.ncount, block / 32), st>>>(pl->dt.c, a);
+    if (pl->dt.large) {
+        // one cluster of up to 8 CTAs per solution, each with a share of the tasks
+        int csize = (a.tasks + 511) / 512;
+        csize = csize < 1 ? 1 : (csize > 8 ? 8 : csize);
+        const int block = choose_block((a.tasks + csize - 1) / csize);
+        const int nw = block / 32;
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(count * csize);
+        cfg.blockDim = dim3(block);
+        cfg.dynamicSmemBytes = (size_t)nw * (4 * mc_ncount_pad((int)pl->dt.ncount) + 2 * sizeof(SwapRecord)) +
+                               2 * sizeof(SwapRecord);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = csize;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        HEA_CUDA(cudaLaunchKernelEx(&cfg, pl->dt.mc, pl->dt.c, a));
+    } else {
+        const int block = choose_block(a.tasks);
+        pl->dt.mc<<<count, block, mc_smem(pl->dt.c.occ_stride, (int)pl->dt.ncount, block / 32), st>>>(pl->dt.c, a);
+    }
     HEA_CUDA(cudaGetLastError());
     if (timed) {
         HEA_CUDA(cudaEventRecord(pl->mc_events[2 * pl->mc_timed + 1], st));
@@ -691,7 +780,7 @@ int plan_create(const hea_problem *pb, const hea_params *prm, int slots, hea_pla
     *out = nullptr;
     hea_plan *pl = new (std::nothrow) hea_plan();
     if (!pl) return fail(HEA_ERR_NOMEM, "out of host memory");
-    int rc = build_tables(pb, prm->seed, pl->dt);
+    int rc = build_tables(pb, prm->seed, pl->dt, prm->flags);
     if (rc == HEA_OK) {
         pl->prm = *prm;
         pl->P = prm->num_solutions;

@@ -1,0 +1,276 @@
+// hea_large.cuh -- the search for structures whose occupancy does not fit in
+// shared memory (up to millions of sites).
+//
+// Same contract as hea_search.cuh (Philox streams, counts, fitness order,
+// ties), so results are bit-identical to the shared-memory path; only where
+// the occupancy lives and how many SMs work on one solution change:
+//   * the occupancy row stays in HBM as 5*species bytes (converted in place at
+//     the start of a local search and back at the end), read through L1;
+//   * one thread-block cluster per solution: the round's tasks are split over
+//     the cluster's CTAs; each CTA reduces its warps' records, publishes its
+//     best in shared memory, and after one cluster barrier every warp reads the
+//     CL records through distributed shared memory and applies the same winner;
+//   * every CTA writes the accepted swap's two bytes itself, so a CTA's L1
+//     never holds a stale copy of its solution's row (the only writes to the
+//     row during the search are those swaps);
+//   * generation and recount are grid-wide over sites (many CTAs per solution).
+#pragma once
+#include <cooperative_groups.h>
+
+#include "hea_search.cuh"
+
+namespace hea {
+
+namespace cg = cooperative_groups;
+
+// Random occupancy of population positions [0, count) of `generation` into
+// slot rows order[pos], as species bytes.  grid = (chunks, count).
+template <int T>
+__global__ void __launch_bounds__(256) large_generate_kernel(const SearchConst c, uint8_t *occ, const int32_t *order,
+                                                             uint32_t generation)
+{
+    const uint32_t pos = blockIdx.y;
+    uint8_t *row = occ + (size_t)order[pos] * c.occ_stride;
+    uint32_t rk[kFeistelRounds];
+    const u32x4 w0 = philox4x32_10(u32x4{pos, generation, 0u, kInitStream}, c.key0, c.key1);
+    const u32x4 w1 = philox4x32_10(u32x4{pos, generation, 1u, kInitStream}, c.key0, c.key1);
+    rk[0] = w0.x; rk[1] = w0.y; rk[2] = w0.z; rk[3] = w0.w; rk[4] = w1.x; rk[5] = w1.y;
+    const int n = c.num_sites;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        uint32_t y = feistel((uint32_t)s, c.feistel_h, rk);
+        while (y >= (uint32_t)n) y = feistel(y, c.feistel_h, rk);
+        int t = 0;
+#pragma unroll
+        for (int i = 1; i < T; ++i) t += (int)(y >= (uint32_t)c.prefix[i]);
+        row[s] = (uint8_t)t;
+    }
+}
+
+// Pair counts of slot rows order[pos] (species bytes), accumulated into
+// cnt[order[pos]] (zeroed by the caller).  grid = (chunks, count); each CTA
+// counts a range of sites into shared bins and adds them once.
+template <int T, int S>
+__global__ void __launch_bounds__(256) large_recount_kernel(const SearchConst c, const int4 *__restrict__ nbor,
+                                                            const uint8_t *occ, const int32_t *order, int32_t *cnt)
+{
+    __shared__ int32_t bins[S * T * T];
+    const int slot = order[blockIdx.y];
+    const uint8_t *row = occ + (size_t)slot * c.occ_stride;
+    for (int x = threadIdx.x; x < S * T * T; x += blockDim.x) bins[x] = 0;
+    __syncthreads();
+    const int n = c.num_sites;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const int a = row[s];
+        const int4 *r = nbor + (size_t)s * c.row4;
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+            uint32_t h = 0;
+            const int4 *seg = r + c.off4[k];
+            for (int ch = 0; ch < c.chunks[k]; ++ch) {
+                const int4 x = __ldg(seg + ch);
+                h += (1u << (5 * row[x.x])) + (1u << (5 * row[x.y])) + (1u << (5 * row[x.z])) + (1u << (5 * row[x.w]));
+            }
+#pragma unroll
+            for (int t = 0; t < T; ++t) {
+                const int v = (int)((h >> (5 * t)) & 31u);
+                if (v) atomicAdd(&bins[(k * T + a) * T + t], v);
+            }
+        }
+    }
+    __syncthreads();
+    int32_t *g = cnt + (size_t)slot * S * T * T;
+    for (int x = threadIdx.x; x < S * T * T; x += blockDim.x) {
+        int v = bins[x];
+        if (blockIdx.x == 0 && x % T == 0) {  // sentinel entries land in field 0: pad_k per site of species i
+            const int k = x / (T * T), i = (x / T) % T;
+            v -= c.pad[k] * (c.prefix[i + 1] - c.prefix[i]);
+        }
+        if (v) atomicAdd(&g[x], v);
+    }
+}
+
+// f2 of slots order[0, count) from their counts.
+template <int T, int S>
+__global__ void large_fitness_kernel(const SearchConst c, const int32_t *order, int count, const int32_t *cnt,
+                                     double *f2)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    const int slot = order[p];
+    f2[slot] = fitness_of_counts<T, S>(c, cnt + (size_t)slot * S * T * T);
+}
+
+// The local search with the occupancy in HBM, one cluster per solution.
+// Shared memory: nwarps * (4 * ncount_pad + 2 * sizeof(SwapRecord)) + 2 * sizeof(SwapRecord).
+template <int T, class L>
+__global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, const McArgs g)
+{
+    constexpr int S = L::S, NC = S * T * T, NCP = mc_ncount_pad(NC);
+    extern __shared__ __align__(16) uint8_t smem[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank(), csize = (int)cluster.num_blocks();
+    const int sol = blockIdx.x / csize;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    int32_t *cnt_all = reinterpret_cast<int32_t *>(smem);
+    int32_t *cnt = cnt_all + warp * NCP;
+    SwapRecord *rec = reinterpret_cast<SwapRecord *>(cnt_all + nwarps * NCP);  // [2][nwarps]
+    SwapRecord *cta_rec = rec + 2 * nwarps;                                      // [2]: this CTA's best
+
+    const int slot = g.order[sol];
+    const uint32_t stream = (g.mc_call << 16) | (uint32_t)sol;
+    uint8_t *row = g.occ + (size_t)slot * c.occ_stride;
+    int32_t *gcnt = g.cnt + (size_t)slot * NC;
+    const int n = c.num_sites;
+    // this CTA's share of the row and of the tasks
+    const int part = (n + csize - 1) / csize, lo = rank * part, hi = min(n, lo + part);
+    const int qpart = (g.tasks + csize - 1) / csize, qlo = rank * qpart, qhi = min(g.tasks, qlo + qpart);
+
+    for (int s = lo + tid; s < hi; s += blockDim.x) row[s] = (uint8_t)(5 * row[s]);
+    for (int x = lane; x < NC; x += 32) cnt[x] = gcnt[x];
+    cluster.sync();
+
+    double cur = g.f2[slot];
+    int miss = 0;
+    int64_t round = 0, accepts = 0, evals = 0;
+    while (miss < g.depth && round < g.max_rounds) {
+        SwapRecord *rr = rec + (round & 1) * nwarps;
+        SwapRecord &mine = rr[warp];
+        if (lane == 0) {
+            mine.f2 = inf_d();
+            mine.task = 0x7FFFFFFF;
+        }
+        __syncwarp();
+        for (int q0 = qlo + warp * 32; q0 < qhi; q0 += blockDim.x) {
+            const int q = q0 + lane;
+            uint32_t s1 = 0, s2 = 0;
+            const bool ok = q < qhi && draw_pair(c, stream, (uint32_t)round, (uint32_t)q, row, s1, s2);
+            __syncwarp();
+            double f = inf_d();
+            uint32_t h1[S], h2[S];
+            int m[S], a = 0, b = 0;
+            if (ok) {
+                ++evals;
+                a = row[s1] / 5;
+                b = row[s2] / 5;
+                f = score_swap<T, L>(c, g.nbor, row, cnt, s1, s2, a, b, h1, h2, m);
+            }
+            double wf = f;
+            int wq = ok ? q : 0x7FFFFFFF;
+            warp_argmin(wf, wq);
+            if (ok && wq == q && better(wf, wq, mine.f2, mine.task)) {
+                SwapRecord r;
+                r.f2 = wf;
+                r.task = wq;
+                r.s1 = s1;
+                r.s2 = s2;
+                r.ab = a | (b << 8);
+                r.m = 0;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    r.h1[k] = k < S ? h1[k < S ? k : 0] : 0;
+                    r.h2[k] = k < S ? h2[k < S ? k : 0] : 0;
+                    if (k < S) r.m |= m[k < S ? k : 0] << (8 * k);
+                }
+                r.pad_ = 0;
+                mine = r;
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        // this CTA's best record, published for the cluster
+        if (warp == 0) {
+            double xf = lane < nwarps ? rr[lane].f2 : inf_d();
+            int xq = lane < nwarps ? rr[lane].task : 0x7FFFFFFF;
+            int xw = lane;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const double of = __shfl_xor_sync(0xFFFFFFFFu, xf, o);
+                const int oq = __shfl_xor_sync(0xFFFFFFFFu, xq, o);
+                const int ow = __shfl_xor_sync(0xFFFFFFFFu, xw, o);
+                if (better(of, oq, xf, xq)) {
+                    xf = of;
+                    xq = oq;
+                    xw = ow;
+                }
+            }
+            if (lane == 0) cta_rec[round & 1] = rr[xw];
+        }
+        cluster.sync();
+        // every warp reduces the cluster's records
+        double xf = inf_d();
+        int xq = 0x7FFFFFFF, xr = 0;
+        if (lane < csize) {
+            const SwapRecord *remote = cluster.map_shared_rank(&cta_rec[round & 1], lane);
+            xf = remote->f2;
+            xq = remote->task;
+            xr = lane;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const double of = __shfl_xor_sync(0xFFFFFFFFu, xf, o);
+            const int oq = __shfl_xor_sync(0xFFFFFFFFu, xq, o);
+            const int orr = __shfl_xor_sync(0xFFFFFFFFu, xr, o);
+            if (better(of, oq, xf, xq)) {
+                xf = of;
+                xq = oq;
+                xr = orr;
+            }
+        }
+        if (xf < cur) {
+            const SwapRecord w = *cluster.map_shared_rank(&cta_rec[round & 1], xr);
+            const int a = w.ab & 0xFF, b = (w.ab >> 8) & 0xFF;
+            row[w.s1] = (uint8_t)(5 * b);  // every CTA writes the swap itself
+            row[w.s2] = (uint8_t)(5 * a);
+            for (int x = lane; x < NC; x += 32) {
+                const int k = x / (T * T), i = (x / T) % T, j = x % T;
+                const uint32_t h1 = w.h1[k], h2 = w.h2[k];
+                const int m = (w.m >> (8 * k)) & 0xFF;
+                const int ui = (int)((h2 >> (5 * i)) & 31u) - (int)((h1 >> (5 * i)) & 31u) + (i == b ? m : 0) -
+                               (i == a ? m : 0);
+                const int uj = (int)((h2 >> (5 * j)) & 31u) - (int)((h1 >> (5 * j)) & 31u) + (j == b ? m : 0) -
+                               (j == a ? m : 0);
+                cnt[x] += ((i == a) - (i == b)) * uj + ((j == a) - (j == b)) * ui;
+            }
+            __syncwarp();
+            if (g.trace && rank == 0 && warp == 0 && accepts < g.trace_cap) {
+                if (lane == 0) {
+                    AcceptRecord r;
+                    r.round = (uint32_t)round;
+                    r.task = (uint32_t)xq;
+                    r.s1 = w.s1;
+                    r.s2 = w.s2;
+                    r.f2 = xf;
+                    g.trace[(size_t)sol * g.trace_cap + accepts] = r;
+                }
+                if (g.trace_counts) {
+                    int32_t *dst = g.trace_counts + ((size_t)sol * g.trace_cap + accepts) * NC;
+                    for (int x = lane; x < NC; x += 32) dst[x] = cnt[x];
+                }
+            }
+            cur = xf;
+            miss = 0;
+            ++accepts;
+        } else {
+            ++miss;
+        }
+        ++round;
+    }
+    cluster.sync();  // every CTA's last reads of the row are done
+    for (int s = lo + tid; s < hi; s += blockDim.x) row[s] = (uint8_t)(row[s] / 5);
+    if (rank == 0 && warp == 0)
+        for (int x = lane; x < NC; x += 32) gcnt[x] = cnt[x];
+    unsigned long long ev = (unsigned long long)evals;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) ev += __shfl_xor_sync(0xFFFFFFFFu, ev, o);
+    if (lane == 0 && ev) atomicAdd(&g.stats[1], ev);
+    if (rank == 0 && tid == 0) {
+        g.f2[slot] = cur;
+        atomicAdd(&g.stats[0], (unsigned long long)round);
+        atomicAdd(&g.stats[2], (unsigned long long)accepts);
+        if (g.trace_len) g.trace_len[sol] = accepts;
+        if (g.rounds_out) g.rounds_out[sol] = round;
+    }
+    cluster.sync();  // keep every CTA's shared memory alive until all remote reads are done
+}
+
+}  // namespace hea

@@ -241,8 +241,16 @@ __device__ __forceinline__ double score_swap(const SearchConst &c, const int4 *_
                 }
         }
     } else {
+        // shell by shell: the next shell's loads overlap this shell's fitness terms
+        double f2 = 0.0;
 #pragma unroll
-        for (int k = 0; k < L::S; ++k) shell_hist<L>(c, r1, r2, occ5, s2, k, h1[k], h2[k], m[k]);
+        for (int k = 0; k < L::S; ++k) {
+            shell_hist<L>(c, r1, r2, occ5, s2, k, h1[k], h2[k], m[k]);
+            int u[T];
+            delta_vector<T>(h1[k], h2[k], m[k], a, b, u);
+            f2 = __fma_rn(c.w[k], shell_error<T>(c, cnt, k, u, a, b), f2);
+        }
+        return f2;
     }
     double f2 = 0.0;
 #pragma unroll
