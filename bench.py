@@ -45,7 +45,11 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["plain_gpu", "plain_cpu", "batched", "large"], default="plain_gpu")
+    ap.add_argument("--workload", choices=["plain_gpu", "plain_cpu", "batched", "large", "serving"],
+                    default="plain_gpu")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="serving: Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-seconds", type=float, default=30.0, help="serving: arrival window, seconds")
+    ap.add_argument("--slice-ms", type=float, default=5.0, help="serving: time slice of one server step")
     ap.add_argument("--large-rounds", type=int, default=4000,
                     help="large workload: cap on rounds per local search (the uncapped search runs for hours)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -289,6 +293,112 @@ def run_large(args):
     return 0
 
 
+def run_serving(args):
+    """Serving loop under a Poisson request stream (workloads.serving): each request an
+    FCC/BCC supercell of 4e3..1e6 sites (log-uniform), 3-6 species, 8 solutions x 256 tasks,
+    4 iterations, depth 10, fitness tolerance 1e-3; tables built on the device from the
+    lattice description.  Requests are submitted at their arrival times while the server
+    runs; latency = arrival to the host holding the result.  value = swap evaluations of
+    the finished requests / wall time of the run."""
+    import math
+
+    import numpy as np
+    import torch
+
+    import pyhea_b200 as hb
+    from pyhea_b200 import workloads as W
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    P, Q, I, D, tol = 8, 256, 4, 10, 1e-3
+    reqs = W.serving(seed=0, rate=args.serve_rate, duration=args.serve_seconds, P=P, Q=Q, I=I, D=D)
+    srv = hb.Server(max_requests=1024, arena_bytes=48 << 30, slice_ms=args.slice_ms)
+    lo, hi = math.log(4e3), math.log(1e6)
+
+    def level(n):  # smaller requests first
+        return min(15, max(0, int(16 * (math.log(n) - lo) / (hi - lo))))
+
+    def submit(st, seed):
+        q = dict(num_solutions=P, total_iter=I, parallel_task=Q, converge_depth=D, seed=seed)
+        return srv.submit_lattice(st.lattice, st.cell, st.species, st.weight, st.target, q, shell_set=st.shell_set,
+                                  tolerance=tol, priority=level(st.num_sites))
+
+    warm = W.serving(seed=1, rate=50.0, duration=1.0, P=P, Q=Q, I=I, D=D)
+    warm = sorted(warm, key=lambda r: r[1].num_sites)[: max(args.warmup, 1)]
+    for k, (_, st) in enumerate(warm):
+        submit(st, 10 ** 6 + k)
+    srv.drain()
+    for rid in list(srv._meta):
+        srv.result(rid)
+    base = srv.status()
+
+    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    sampler.start()
+    arrival, size, lat, evals, bytes_alg, iters, h2d, d2h = {}, {}, [], 0, 0.0, [], 0, 0
+    i, t0 = 0, time.perf_counter()
+    hard_stop = args.serve_seconds + 120.0
+    last_done = 0.0
+    while True:
+        now = time.perf_counter() - t0
+        while i < len(reqs) and reqs[i][0] <= now:
+            st = reqs[i][1]
+            rid = submit(st, i)
+            arrival[rid], size[rid] = reqs[i][0], (st.num_sites, st.evals_bytes())
+            h2d += st.species.nbytes + st.weight.nbytes + st.target.nbytes
+            i += 1
+        if i == len(reqs) and not arrival:
+            break
+        if now > hard_stop:
+            break
+        if not arrival:
+            time.sleep(max(0.0, min(reqs[i][0] - now, 0.002)))
+            continue
+        srv.step()
+        for rid in list(arrival):
+            r = srv.result(rid)
+            if r is None:
+                continue
+            occ, fit, info = r
+            t = time.perf_counter() - t0
+            lat.append((t - arrival.pop(rid)) * 1000.0)
+            n, B = size.pop(rid)
+            evals += info["evals"]
+            bytes_alg += info["evals"] * B
+            iters.append(info["iterations"])
+            d2h += occ.nbytes + fit.nbytes
+            last_done = t
+    clocks = sampler.stop()
+    st_end = srv.status()
+    busy = st_end["busy_ms"] - base["busy_ms"]
+    srv.close()
+    wall = last_done
+    lat_a = np.array(lat) if lat else np.array([float("nan")])
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_alg / (busy / 1000.0) / 1e9 if busy > 0 else 0.0
+    value = evals / wall if wall > 0 else 0.0
+    line = {"metric": "swap_evals_per_sec", "value": value, "unit": "swap-evals/s", "n_gpus": 1, "steps": 1,
+            "warmup": len(warm), "ms_per_step": wall * 1000.0, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "serving: Poisson stream of FCC/BCC requests, 4e3..1e6 sites (log-uniform)",
+                       "rate_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds,
+                       "solutions": P, "parallel_task": Q, "total_iter": I, "converge_depth": D, "tolerance": tol,
+                       "slice_ms": args.slice_ms, "priority": "smaller requests first (16 levels by log size)",
+                       "l2": "inputs larger than L2 (tables of the requests on the device exceed 126 MB)"},
+            "requests": {"arrived": i, "finished": len(lat), "unfinished": len(arrival),
+                         "per_s": len(lat) / wall if wall > 0 else 0.0,
+                         "latency_ms": {"p50": float(np.percentile(lat_a, 50)), "p90": float(np.percentile(lat_a, 90)),
+                                        "p99": float(np.percentile(lat_a, 99)), "max": float(lat_a.max())},
+                         "reached_tolerance_before_last_iteration": int(sum(1 for k in iters if k < I))},
+            "gpu_busy_fraction": busy / (wall * 1000.0) if wall > 0 else 0.0,
+            "e2e": {"value": value, "unit": "swap-evals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "note": "the serving line is end to end: one step = the whole run"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "kernel": "batch_kernel (persistent job engine)",
+                         "peak_kind": peak_kind, "traffic": None},
+            "gpu_launches": int(st_end["launches"] - base["launches"]), "clocks": clocks}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -297,6 +407,8 @@ def main():
         return run_batched(args)
     if args.workload == "large":
         return run_large(args)
+    if args.workload == "serving":
+        return run_serving(args)
 
     import numpy as np
     import torch

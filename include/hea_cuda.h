@@ -123,6 +123,75 @@ int hea_batch_finish_times(hea_batch *batch, double *out_ms);
 void hea_batch_destroy(hea_batch *batch);
 
 /*
+ * Serving loop: structure-search requests admitted while others run.  No
+ * counterpart in the reference, whose engine searches one structure per call
+ * (accelerate.cu:1112-1242).  Without a tolerance a request's result is
+ * identical to hea_run_local_parallel_hcs on it alone with the same seed;
+ * with one, to the same request served alone.  Neither depends on what else
+ * was on the GPU or where the time slices fell.
+ *
+ * submit queues a request on the host (inputs are copied); step admits queued
+ * requests in submission order while a request slot, device memory in the
+ * arena and job-ring room are free, runs the persistent search kernel for one
+ * time slice (slice_ms, or until nothing is active), and collects the requests
+ * that finished; result hands over a finished request's population (ascending
+ * fitness) and releases it.  tolerance >= 0 (on the reported fitness, sqrt
+ * of f2): a local search ends once its fitness is <= tolerance, and the
+ * request ends once the best fitness after an iteration's survivors' sort
+ * is; < 0 runs total_iter iterations.  priority 0..15, 0 first.
+ * submit_lattice builds the FCC/BCC table on the device (as
+ * hea_build_neighbors; the first num_shells shells are searched).
+ * result returns HEA_PENDING while the request is queued or running.
+ * Not thread-safe: one host thread drives a server.
+ */
+#define HEA_PENDING 5 /* hea_server_result: the request has not finished */
+
+typedef struct hea_server_config {
+    int32_t max_requests;  /* requests on the device at once (0: 256)                            */
+    int32_t ring_jobs;     /* job-ring slots per priority level (0: 65536)                        */
+    int64_t arena_bytes;   /* device memory for tables and populations (0: 8 GiB or half the free memory) */
+    int32_t smem_bytes;    /* shared memory per CTA; larger structures keep occupancy in HBM (0: auto) */
+    int32_t hbm_sites;     /* structures with at least this many sites keep occupancy in HBM too (0: none) */
+    double slice_ms;       /* length of one step's launch (0: 10 ms)                             */
+} hea_server_config;
+
+typedef struct hea_request_info {
+    int32_t state;        /* 0 queued, 1 on the device, 2 finished, 3 failed                      */
+    int32_t iterations;   /* iterations run (< total_iter when the tolerance was reached)           */
+    int32_t hbm;          /* 1: occupancy kept in HBM                                              */
+    int32_t pad_;
+    double submit_ms;     /* host clock, ms since the server was created                            */
+    double admit_ms;
+    double finish_ms;     /* step end at which the finish was collected                             */
+    double device_ms;     /* device clock from the server's start to the request's final sort       */
+    int64_t rounds, evals, accepts;
+    int64_t device_bytes; /* arena bytes the request held                                           */
+} hea_request_info;
+
+typedef struct hea_server_status {
+    int32_t queued, running, finished_unread, slots_free;
+    int64_t arena_free_bytes, arena_bytes;
+    int64_t rounds, evals, accepts, finished; /* cumulative */
+    double busy_ms;                           /* sum of the step launches' device time */
+    int32_t launches, smem_bytes;
+} hea_server_status;
+
+typedef struct hea_server hea_server;
+int hea_server_create(const hea_server_config *config, hea_server **out);
+int hea_server_submit(hea_server *server, const hea_problem *problem, const hea_params *params, double tolerance,
+                      int32_t priority, int64_t *out_id);
+int hea_server_submit_lattice(hea_server *server, int32_t lattice, int32_t cell, int32_t shell_set,
+                              int32_t num_types, int32_t num_shells, const int32_t *species, const double *weight,
+                              const double *target_sro, const hea_params *params, double tolerance,
+                              int32_t priority, int64_t *out_id);
+int hea_server_step(hea_server *server, int32_t *out_finished);
+int hea_server_result(hea_server *server, int64_t id, uint8_t *out_occ, double *out_fitness,
+                      hea_request_info *info);
+int hea_server_info(hea_server *server, int64_t id, hea_request_info *info);
+int hea_server_status_get(hea_server *server, hea_server_status *status);
+void hea_server_destroy(hea_server *server);
+
+/*
  * Component entry points (host buffers), one launch each, used to check the
  * pieces of the search against the CPU restatement.
  *

@@ -26,7 +26,7 @@ _P = ctypes.POINTER
 _i32, _i64, _u32, _u64, _f64, _u8 = (ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32, ctypes.c_uint64,
                                      ctypes.c_double, ctypes.c_uint8)
 
-HEA_OK, HEA_ERR_INVALID, HEA_ERR_UNSUPPORTED, HEA_ERR_CUDA, HEA_ERR_NOMEM = 0, 1, 2, 3, 4
+HEA_OK, HEA_ERR_INVALID, HEA_ERR_UNSUPPORTED, HEA_ERR_CUDA, HEA_ERR_NOMEM, HEA_PENDING = 0, 1, 2, 3, 4, 5
 HEA_FLAG_LOG_ITERS = 1
 HEA_FLAG_TIME_KERNELS = 2
 HEA_FLAG_HBM_OCCUPANCY = 4
@@ -69,6 +69,29 @@ class AcceptRecord(ctypes.Structure):
     _fields_ = [("round", _u32), ("task", _u32), ("s1", _u32), ("s2", _u32), ("f2", _f64)]
 
 
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("max_requests", _i32), ("ring_jobs", _i32), ("arena_bytes", _i64), ("smem_bytes", _i32),
+                ("hbm_sites", _i32), ("slice_ms", _f64)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("state", _i32), ("iterations", _i32), ("hbm", _i32), ("pad_", _i32), ("submit_ms", _f64),
+                ("admit_ms", _f64), ("finish_ms", _f64), ("device_ms", _f64), ("rounds", _i64), ("evals", _i64),
+                ("accepts", _i64), ("device_bytes", _i64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad_"}
+
+
+class ServerStatus(ctypes.Structure):
+    _fields_ = [("queued", _i32), ("running", _i32), ("finished_unread", _i32), ("slots_free", _i32),
+                ("arena_free_bytes", _i64), ("arena_bytes", _i64), ("rounds", _i64), ("evals", _i64),
+                ("accepts", _i64), ("finished", _i64), ("busy_ms", _f64), ("launches", _i32), ("smem_bytes", _i32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def _declare(lib):
     sig = {
         "hea_cuda_available": (_i32, []),
@@ -89,6 +112,15 @@ def _declare(lib):
         "hea_batch_read": (_i32, [ctypes.c_void_p, _i32, _P(_u8), _P(_f64)]),
         "hea_batch_finish_times": (_i32, [ctypes.c_void_p, _P(_f64)]),
         "hea_batch_destroy": (None, [ctypes.c_void_p]),
+        "hea_server_create": (_i32, [_P(_ServerConfig), _P(ctypes.c_void_p)]),
+        "hea_server_submit": (_i32, [ctypes.c_void_p, _P(_Problem), _P(_Params), _f64, _i32, _P(_i64)]),
+        "hea_server_submit_lattice": (_i32, [ctypes.c_void_p, _i32, _i32, _i32, _i32, _i32, _P(_i32), _P(_f64),
+                                             _P(_f64), _P(_Params), _f64, _i32, _P(_i64)]),
+        "hea_server_step": (_i32, [ctypes.c_void_p, _P(_i32)]),
+        "hea_server_result": (_i32, [ctypes.c_void_p, _i64, _P(_u8), _P(_f64), _P(RequestInfo)]),
+        "hea_server_info": (_i32, [ctypes.c_void_p, _i64, _P(RequestInfo)]),
+        "hea_server_status_get": (_i32, [ctypes.c_void_p, _P(ServerStatus)]),
+        "hea_server_destroy": (None, [ctypes.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -233,6 +265,104 @@ class Batch:
     def close(self):
         if self._h:
             lib.hea_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Serving loop (hea_server_*): searches submitted while others run.
+
+    ``submit`` / ``submit_lattice`` queue a request and return its id;
+    ``step`` admits queued requests as request slots, arena memory and job-ring
+    room free up, runs one time slice of the persistent kernel and returns the
+    ids that finished; ``result`` hands over (occupancies [P][N] ascending by
+    fitness, fitness [P], info dict) once and releases the request.  A request's
+    result equals search() on it alone with the same seed (with a tolerance:
+    with total_iter = info["iterations"])."""
+
+    def __init__(self, max_requests=0, ring_jobs=0, arena_bytes=0, smem_bytes=0, slice_ms=0.0, hbm_sites=0):
+        cfg = _ServerConfig(int(max_requests), int(ring_jobs), int(arena_bytes), int(smem_bytes), int(hbm_sites),
+                            float(slice_ms))
+        self._h = ctypes.c_void_p()
+        _check(lib.hea_server_create(ctypes.byref(cfg), ctypes.byref(self._h)))
+        self._meta = {}  # id -> (P, N)
+
+    @staticmethod
+    def _prm(params):
+        return _params(params["num_solutions"], params["total_iter"], params["parallel_task"],
+                       params["converge_depth"], params.get("seed", 0), params.get("max_rounds", 0))
+
+    def submit(self, problem, params, tolerance=-1.0, priority=0):
+        prm = self._prm(params)
+        rid = _i64()
+        _check(lib.hea_server_submit(self._h, ctypes.byref(problem._c), ctypes.byref(prm), float(tolerance),
+                                     int(priority), ctypes.byref(rid)))
+        self._meta[rid.value] = (int(params["num_solutions"]), problem.num_sites)
+        return rid.value
+
+    def submit_lattice(self, lattice, cell, species, weight, target_sro, params, shell_set=SHELLS_REFERENCE,
+                       tolerance=-1.0, priority=0):
+        sp = np.ascontiguousarray(species, dtype=np.int32)
+        w = np.ascontiguousarray(weight, dtype=np.float64)
+        tg = np.ascontiguousarray(target_sro, dtype=np.float64)
+        T, S = sp.size, w.size
+        if tg.size != S * T * T:
+            raise ValueError(f"target_sro needs {S}*{T}*{T} values, got {tg.size}")
+        prm = self._prm(params)
+        rid = _i64()
+        _check(lib.hea_server_submit_lattice(self._h, int(lattice), int(cell), int(shell_set), T, S, _ptr(sp, _i32),
+                                             _ptr(w, _f64), _ptr(tg, _f64), ctypes.byref(prm), float(tolerance),
+                                             int(priority), ctypes.byref(rid)))
+        n = (4 if lattice == FCC else 2) * int(cell) ** 3
+        self._meta[rid.value] = (int(params["num_solutions"]), n)
+        return rid.value
+
+    def step(self):
+        """One admission + time slice + collection; returns the number of requests that finished."""
+        fin = _i32()
+        _check(lib.hea_server_step(self._h, ctypes.byref(fin)))
+        return fin.value
+
+    def info(self, rid):
+        inf = RequestInfo()
+        _check(lib.hea_server_info(self._h, int(rid), ctypes.byref(inf)))
+        return inf.as_dict()
+
+    def result(self, rid):
+        """(occ, fitness, info) of a finished request, or None while it is queued or running."""
+        P, n = self._meta.get(rid, (0, 0))
+        occ = np.empty((P, n), dtype=np.uint8)
+        fit = np.empty(P, dtype=np.float64)
+        inf = RequestInfo()
+        rc = lib.hea_server_result(self._h, int(rid), _ptr(occ, _u8), _ptr(fit, _f64), ctypes.byref(inf))
+        if rc == HEA_PENDING:
+            return None
+        self._meta.pop(rid, None)
+        _check(rc)
+        return occ, fit, inf.as_dict()
+
+    def status(self):
+        st = ServerStatus()
+        _check(lib.hea_server_status_get(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def drain(self, max_steps=1 << 30):
+        """Step until nothing is queued or running."""
+        for _ in range(max_steps):
+            st = self.status()
+            if st["queued"] == 0 and st["running"] == 0:
+                return
+            self.step()
+        raise HeaError(HEA_ERR_CUDA, "server did not drain")
+
+    def close(self):
+        if self._h:
+            lib.hea_server_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

@@ -1,9 +1,12 @@
-// hea_batch.cuh -- many independent structures in one persistent kernel.
+// hea_batch.cuh -- the job engine: many independent structures searched by one
+// persistent kernel.  It serves both the batch API (hea_batch_*: a fixed set
+// of structures in one graph-captured launch) and the serving loop
+// (hea_server_*: structures admitted while others run, in time slices).
 //
 // Every structure runs the same search as the plain path (hea_search.cuh) with
 // its own constants, tables, population pools and Philox key, so its result
-// is bit-identical to searching it alone.  The work of all structures is a
-// queue of jobs in HBM:
+// is bit-identical to searching it alone, whatever else shares the GPU.  Its
+// work is a sequence of phases of jobs:
 //
 //   phase 0        P x GEN0 (generation 0 of the population) and, when I > 0,
 //                  P x GENMC(0) (generation 1 of the new population, then its
@@ -14,15 +17,31 @@
 //
 // The CTA that finishes the last job of a structure's phase runs the phase
 // transition itself -- stable sort of the survivors, then the merge
-// (pyhea/cpp/accelerate.cpp:305-330, :693) -- and appends the next phase's jobs.
-// Structures are ranked by work (sites x solutions x iterations) into
-// kBatchLevels queues; a CTA takes the next published job of the highest
-// level that has one, so the largest structures -- the longest chains of
-// dependent phases -- advance first, a few at a time (their neighbour tables
-// then stay in L2), and the smaller ones fill the gaps.  Each
-// queue's slot count is known in advance (P (2I + 1) per structure); a CTA
-// exits once every slot of every queue has been taken.  Waits are bounded by
-// wall time; on expiry the kernel sets an error flag and every CTA returns.
+// (pyhea/cpp/accelerate.cpp:305-330, :693) -- and appends the next phase's
+// jobs.  With a tolerance, a local search also ends once its f2 is at or
+// below it, and the structure ends once the best f2 after a survivors' sort
+// is (the search of the population generated meanwhile is dropped).
+//
+// Jobs live in ring queues, one per priority level, whose head and tail only
+// grow; a CTA takes the next reserved job of the highest level that has one
+// and waits for the producer's sequence number in the slot.  A ring needs
+// room for the jobs of one phase of every structure at its level (at most
+// 2P each), since a phase is queued only after the previous one finished.
+//
+// A launch ends when no structure is active or, for the time slices of the
+// serving loop, at its deadline: CTAs stop taking jobs, and a local search
+// that sees the deadline stops at the end of its round, saves its state
+// (occupancy, counts, f2) to HBM and queues a continuation that resumes at
+// the next round with the same rejection count -- the same proposals follow,
+// so the result does not depend on where the slices fell.  Waits are bounded
+// by wall time since the last finished job; on expiry the kernel sets an
+// error flag and every CTA returns.
+//
+// Structures whose occupancy does not fit the launch's shared memory keep it
+// in HBM (`hbm`): a job converts the row to 5*species in place (reads through
+// L2, so no stale L1 line of another SM's writes is used; the conversion
+// rewrites every byte this CTA later reads), searches it through L1, and
+// converts it back.
 #pragma once
 #include <cstdint>
 
@@ -34,9 +53,11 @@ enum BatchJobKind : int32_t { kJobGen0 = 0, kJobGenMc = 1, kJobMc2 = 2 };
 
 struct BatchJob {
     int32_t structure, kind, index, iter;
-    int32_t ready;  // 1 once the fields above are visible
-    int32_t pad_[3];
+    int32_t seq;     // low 32 bits of (ring position + 1), written after the other fields
+    int32_t resume;  // 1: continue a stopped local search at round0 with miss0 rejections
+    int32_t round0, miss0;
 };
+static_assert(sizeof(BatchJob) == 32, "BatchJob layout");
 
 // Kernel instance of a structure: species count and shell layout.
 enum BatchLayout : int32_t { kLayBcc = 0, kLayFccTrue = 1, kLayRt1 = 2, kLayRt2 = 3, kLayRt3 = 4 };
@@ -51,40 +72,39 @@ struct BatchStruct {
     int32_t *scratch;  // [2P] sort scratch
     int32_t P, Q, D, I;
     int64_t max_rounds;
-    int32_t T, layout, level, pad_;
+    double tol2;  // tolerance on f2 (< 0: none): local searches and the structure end once reached
+    int32_t T, layout, level, hbm;
 };
 
 static_assert(sizeof(SearchConst) % 8 == 0 && alignof(SearchConst) >= 8, "SearchConst copied as 8-byte words");
 
 struct BatchState {
     int32_t remaining;  // jobs of the current phase not finished
-    int32_t phase;
+    int32_t phase;      // at the end: the iterations run
+    int32_t done;       // 1 once the structure's search ended
+    int32_t pad_;
+    unsigned long long tally[3];  // rounds, evals, accepts of this structure
 };
 
 constexpr int kBatchLevels = 16;
 
 struct BatchQueue {
-    unsigned long long head;   // slots taken
-    unsigned long long tail;   // slots reserved by producers
-    unsigned long long total;  // slots this queue will ever hold
-    unsigned long long base;   // first slot of this queue in the job array
+    unsigned long long head;  // jobs taken
+    unsigned long long tail;  // jobs reserved by producers
+    unsigned long long cap;   // ring slots
+    unsigned long long base;  // first slot of this ring in the job array
 };
 
 struct BatchCtl {
     BatchQueue q[kBatchLevels];
     unsigned long long stats[4];  // rounds, evals, accepts, finished structures
-    int32_t error;                // 1: a wait ran out of time
-    int32_t pad_;
+    int32_t error;                // 1: a wait ran out of time, 2: a ring slot was overwritten
+    int32_t active;               // structures seeded and not finished
     unsigned long long wait_limit_ns;
-    unsigned long long start_ns;  // device clock when the phase-0 jobs were queued
+    unsigned long long start_ns;     // device time origin of finish times
+    unsigned long long deadline_ns;  // device time after which no job starts (0: none)
+    unsigned long long progress_ns;  // device time of the last finished job
 };
-
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
 
 // Stable ascending order of order[0, count) by f2 (rank counting); block-wide,
 // barriers inside.  scratch holds `count` ints.  Reads go through L2: the
@@ -106,46 +126,78 @@ __device__ __forceinline__ void block_stable_sort(int32_t *order, const double *
     __syncthreads();
 }
 
-// Append `n` jobs of one kind for structure s to queue `level` (block-wide;
-// thread 0 reserves the slots).
-__device__ __forceinline__ void enqueue_jobs(BatchJob *jobs, BatchCtl *ctl, int level, int s, int kind, int iter,
-                                             int n, unsigned long long *base_sh)
+__device__ __forceinline__ BatchJob &ring_slot(BatchJob *jobs, const BatchQueue &q, unsigned long long h)
 {
-    if (threadIdx.x == 0) *base_sh = ctl->q[level].base + atomicAdd(&ctl->q[level].tail, (unsigned long long)n);
+    return jobs[q.base + h % q.cap];
+}
+
+// Append `n` fresh jobs of one kind for structure s to ring `level`
+// (block-wide; thread 0 reserves the positions).
+__device__ __forceinline__ void enqueue_jobs(BatchJob *jobs, BatchCtl *ctl, int level, int s, int kind, int iter,
+                                             int n, unsigned long long *first_sh)
+{
+    if (threadIdx.x == 0) *first_sh = atomicAdd(&ctl->q[level].tail, (unsigned long long)n);
     __syncthreads();
-    const unsigned long long base = *base_sh;
+    const unsigned long long first = *first_sh;
+    const BatchQueue &q = ctl->q[level];
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        BatchJob &j = jobs[base + i];
+        const unsigned long long h = first + i;
+        BatchJob &j = ring_slot(jobs, q, h);
         j.structure = s;
         j.kind = kind;
         j.index = i;
         j.iter = iter;
+        j.resume = 0;
+        j.round0 = 0;
+        j.miss0 = 0;
         __threadfence();
-        atomicExch(&j.ready, 1);
+        atomicExch(&j.seq, (int32_t)(uint32_t)(h + 1));
     }
     __syncthreads();
 }
 
-// Thread 0: take the next reserved slot of the highest level that has one.
-// Returns the slot, or -1 when every slot of every queue is taken (or on error).
-__device__ __forceinline__ long long claim_job(BatchCtl *ctl)
+// Thread 0: the continuation of a stopped local search.
+__device__ __forceinline__ void enqueue_resume(BatchJob *jobs, BatchCtl *ctl, int level, const BatchJob &job,
+                                               int64_t round0, int miss0)
+{
+    const unsigned long long h = atomicAdd(&ctl->q[level].tail, 1ull);
+    BatchJob &j = ring_slot(jobs, ctl->q[level], h);
+    j.structure = job.structure;
+    j.kind = job.kind;
+    j.index = job.index;
+    j.iter = job.iter;
+    j.resume = 1;
+    j.round0 = (int32_t)round0;
+    j.miss0 = miss0;
+    __threadfence();
+    atomicExch(&j.seq, (int32_t)(uint32_t)(h + 1));
+}
+
+// Thread 0: take the next reserved job of the highest level that has one.
+// Returns its slot and expected sequence number, or -1 when no structure is
+// active, the deadline has passed, or on error.
+__device__ __forceinline__ long long claim_job(BatchCtl *ctl, unsigned long long deadline, int32_t *seq)
 {
     const unsigned long long t0 = global_ns();
     for (;;) {
-        bool left = false;
+        if (*(volatile int32_t *)&ctl->active <= 0 || *(volatile int32_t *)&ctl->error) return -1;
+        const unsigned long long now = global_ns();
+        if (deadline && now >= deadline) return -1;
         for (int l = 0; l < kBatchLevels; ++l) {
             volatile BatchQueue *q = &ctl->q[l];
             unsigned long long h = q->head;
-            if (h < q->total) left = true;
             while (h < q->tail) {
                 const unsigned long long old = atomicCAS(&ctl->q[l].head, h, h + 1);
-                if (old == h) return (long long)(q->base + h);
+                if (old == h) {
+                    *seq = (int32_t)(uint32_t)(h + 1);
+                    return (long long)(q->base + h % q->cap);
+                }
                 h = old;
             }
         }
-        if (!left) return -1;
-        if (*(volatile int32_t *)&ctl->error) return -1;
-        if (global_ns() - t0 > ctl->wait_limit_ns) {
+        const unsigned long long prog = *(volatile unsigned long long *)&ctl->progress_ns;
+        const unsigned long long since = prog > t0 ? prog : t0;  // another SM's clock read may be ahead of ours
+        if (now > since && now - since > ctl->wait_limit_ns) {
             atomicExch(&ctl->error, 1);
             return -1;
         }
@@ -153,63 +205,76 @@ __device__ __forceinline__ long long claim_job(BatchCtl *ctl)
     }
 }
 
-// Initial jobs of every structure (phase 0); one CTA per structure.
-__global__ void batch_seed_kernel(BatchStruct *structs, BatchState *states, BatchJob *jobs, BatchCtl *ctl)
+// Phase-0 jobs of structures list[0, gridDim.x) (all structures when list is
+// NULL); one CTA per structure.
+__global__ void batch_seed_kernel(const BatchStruct *structs, const int32_t *list, BatchState *states, BatchJob *jobs,
+                                  BatchCtl *ctl)
 {
-    __shared__ unsigned long long base;
-    const int s = blockIdx.x;
-    if (s == 0 && threadIdx.x == 0) ctl->start_ns = global_ns();
+    __shared__ unsigned long long first;
+    const int s = list ? list[blockIdx.x] : (int)blockIdx.x;
     const BatchStruct &d = structs[s];
     if (threadIdx.x == 0) {
-        states[s].phase = 0;
-        states[s].remaining = d.I > 0 ? 2 * d.P : d.P;
+        BatchState &st = states[s];
+        st.remaining = d.I > 0 ? 2 * d.P : d.P;
+        st.phase = 0;
+        st.done = 0;
+        st.tally[0] = st.tally[1] = st.tally[2] = 0;
+        __threadfence();
+        atomicAdd(&ctl->active, 1);
     }
     for (int i = threadIdx.x; i < 2 * d.P; i += blockDim.x) d.order[i] = i;
     __syncthreads();
-    enqueue_jobs(jobs, ctl, d.level, s, kJobGen0, 0, d.P, &base);
-    if (d.I > 0) enqueue_jobs(jobs, ctl, d.level, s, kJobGenMc, 0, d.P, &base);
+    enqueue_jobs(jobs, ctl, d.level, s, kJobGen0, 0, d.P, &first);
+    if (d.I > 0) enqueue_jobs(jobs, ctl, d.level, s, kJobGenMc, 0, d.P, &first);
 }
 
+struct JobEnd {
+    int32_t yielded, round, miss;
+};
+
 // One job of a structure with species count T and layout L.  Shared memory:
-// occ5 (occ_stride + 16) | per-warp counts | swap records.
+// [occ5 (occ_stride + 16), unless hbm] | per-warp counts | swap records.
 #ifndef HEA_BATCH_AHEAD
 #define HEA_BATCH_AHEAD true  // whole-row loads before use (the batch kernel has 128 registers per thread)
 #endif
 template <int T, class L>
-__device__ __noinline__ void batch_job(const SearchConst &c, const BatchStruct &d, const BatchJob &job, uint8_t *smem,
-                                       unsigned long long *stats)
+__device__ __noinline__ JobEnd batch_job(const SearchConst &c, const BatchStruct &d, const BatchJob &job,
+                                         uint8_t *smem, unsigned long long *stats, unsigned long long *tally,
+                                         unsigned long long deadline)
 {
     constexpr int S = L::S, NC = S * T * T, NCP = mc_ncount_pad(NC);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    uint8_t *occ5 = smem;
-    int32_t *cnt_all = reinterpret_cast<int32_t *>(smem + c.occ_stride + 16);
-    SwapRecord *rec = reinterpret_cast<SwapRecord *>(cnt_all + nwarps * NCP);
-    const int P = d.P;
+    const bool hbm = d.hbm != 0;
+    const int P = d.P, n = c.num_sites;
     const int pos = job.index;
     const int slot = __ldcg(d.order + (job.kind == kJobGenMc ? P + pos : pos));
     uint8_t *gocc = d.occ + (size_t)slot * c.occ_stride;
     int32_t *gcnt = d.cnt + (size_t)slot * NC;
+    uint8_t *occ5 = hbm ? gocc : smem;
+    int32_t *cnt_all = reinterpret_cast<int32_t *>(hbm ? smem : smem + c.occ_stride + 16);
+    SwapRecord *rec = reinterpret_cast<SwapRecord *>(cnt_all + nwarps * NCP);
 
     double cur;
-    if (job.kind == kJobMc2) {
-        stage_occupancy<true>(c, gocc, occ5);
+    if (job.kind == kJobMc2 || job.resume) {
+        stage_occupancy<true>(c, gocc, occ5);  // in place when hbm
         for (int x = lane; x < NC; x += 32) cnt_all[warp * NCP + x] = __ldcg(gcnt + x);
         __syncthreads();
-        if (threadIdx.x == 0) occ5[c.num_sites] = 0;
+        if (threadIdx.x == 0) occ5[n] = 0;  // sentinel
         cur = __ldcg(d.f2 + slot);
         __syncthreads();
     } else {
         const uint32_t generation = job.kind == kJobGen0 ? 0u : (uint32_t)(job.iter + 1);
-        generate_occupancy<T>(c, (uint32_t)pos, generation, occ5, job.kind == kJobGen0 ? gocc : nullptr);
-        if (threadIdx.x == 0) occ5[c.num_sites] = 0;
+        generate_occupancy<T>(c, (uint32_t)pos, generation, occ5, (job.kind == kJobGen0 && !hbm) ? gocc : nullptr);
+        if (threadIdx.x == 0) occ5[n] = 0;
         __syncthreads();
         block_recount<T, S>(c, d.nbor, occ5, cnt_all);  // copy 0; ends with a barrier
         cur = fitness_of_counts<T, S>(c, cnt_all);
         if (job.kind == kJobGen0) {
+            if (hbm) unstage_occupancy(c, occ5, gocc);
             if (warp == 0)
                 for (int x = lane; x < NC; x += 32) gcnt[x] = cnt_all[x];
             if (threadIdx.x == 0) d.f2[slot] = cur;
-            return;
+            return JobEnd{0, 0, 0};
         }
         for (int x = lane; x < NC; x += 32)
             if (warp) cnt_all[warp * NCP + x] = cnt_all[x];
@@ -217,26 +282,29 @@ __device__ __noinline__ void batch_job(const SearchConst &c, const BatchStruct &
     }
     const uint32_t call = job.kind == kJobMc2 ? (uint32_t)(2 * job.iter + 1) : (uint32_t)(2 * job.iter);
     const uint32_t stream = (call << 16) | (uint32_t)pos;
-    const McTally t =
-        mc_rounds<T, L, HEA_BATCH_AHEAD>(c, d.nbor, occ5, cnt_all, rec, stream, cur, d.Q, d.D, d.max_rounds,
-                                         McTrace{nullptr, nullptr, 0});
-    unstage_occupancy(c, occ5, gocc);
+    const McResume rs{job.resume ? (int64_t)job.round0 : 0, job.resume ? job.miss0 : 0, deadline, d.tol2};
+    const McTally t = mc_rounds<T, L, HEA_BATCH_AHEAD, true>(c, d.nbor, occ5, cnt_all, rec, stream, cur, d.Q, d.D,
+                                                             d.max_rounds, McTrace{nullptr, nullptr, 0}, rs);
+    unstage_occupancy(c, occ5, gocc);  // in place when hbm
     if (warp == 0)
         for (int x = lane; x < NC; x += 32) gcnt[x] = cnt_all[x];
     add_tally(t, stats);
+    add_tally(t, tally);
     if (threadIdx.x == 0) d.f2[slot] = t.f2;
+    return JobEnd{t.yielded ? 1 : 0, (int32_t)t.round_end, t.miss};
 }
 
 template <int T>
-__device__ __forceinline__ void batch_dispatch_t(const SearchConst &c, const BatchStruct &d, const BatchJob &job,
-                                                 uint8_t *smem, unsigned long long *stats)
+__device__ __forceinline__ JobEnd batch_dispatch_t(const SearchConst &c, const BatchStruct &d, const BatchJob &job,
+                                                   uint8_t *smem, unsigned long long *stats, unsigned long long *tally,
+                                                   unsigned long long deadline)
 {
     switch (d.layout) {
-    case kLayBcc: batch_job<T, Shells<2, 2, 3>>(c, d, job, smem, stats); break;
-    case kLayFccTrue: batch_job<T, Shells<3, 2, 6>>(c, d, job, smem, stats); break;
-    case kLayRt1: batch_job<T, RuntimeShells<1>>(c, d, job, smem, stats); break;
-    case kLayRt2: batch_job<T, RuntimeShells<2>>(c, d, job, smem, stats); break;
-    default: batch_job<T, RuntimeShells<3>>(c, d, job, smem, stats); break;
+    case kLayBcc: return batch_job<T, Shells<2, 2, 3>>(c, d, job, smem, stats, tally, deadline);
+    case kLayFccTrue: return batch_job<T, Shells<3, 2, 6>>(c, d, job, smem, stats, tally, deadline);
+    case kLayRt1: return batch_job<T, RuntimeShells<1>>(c, d, job, smem, stats, tally, deadline);
+    case kLayRt2: return batch_job<T, RuntimeShells<2>>(c, d, job, smem, stats, tally, deadline);
+    default: return batch_job<T, RuntimeShells<3>>(c, d, job, smem, stats, tally, deadline);
     }
 }
 
@@ -244,11 +312,10 @@ __device__ __forceinline__ void batch_dispatch_t(const SearchConst &c, const Bat
 #define HEA_BATCH_THREADS 256
 #endif
 
-// The persistent kernel: CTAs claim job slots in order until every slot is
-// done.  Dynamic shared memory: the largest structure's occupancy + 16 +
-// per-warp counts + swap records; the job's constants (1.9 KB) are copied to
-// static shared memory, which still leaves two CTAs per SM for 108 000-site
-// structures.
+// The persistent kernel: CTAs take jobs until no structure is active or the
+// launch's deadline has passed.  Dynamic shared memory: occupancy of the
+// largest shared-memory structure + 16 + per-warp counts + swap records; the
+// job's constants (1.9 KB) are copied to static shared memory.
 __global__ void __launch_bounds__(HEA_BATCH_THREADS, 2)
     batch_kernel(const BatchStruct *__restrict__ structs, BatchState *states, BatchJob *jobs, BatchCtl *ctl,
                  unsigned long long *finish_ns)
@@ -256,20 +323,22 @@ __global__ void __launch_bounds__(HEA_BATCH_THREADS, 2)
     extern __shared__ __align__(16) uint8_t smem[];
     __shared__ BatchJob job;
     __shared__ int stop, last, phase;
-    __shared__ unsigned long long base;
+    __shared__ unsigned long long first;
     __shared__ __align__(16) SearchConst c;  // this job's constants: fitness tables read from shared memory
+    const unsigned long long deadline = ctl->deadline_ns;  // set before the launch
     for (;;) {
         if (threadIdx.x == 0) {
             stop = 0;
-            const long long h = claim_job(ctl);
+            int32_t seq = 0;
+            const long long h = claim_job(ctl, deadline, &seq);
             if (h < 0) {
                 stop = 1;
             } else {
-                volatile int32_t *ready = &jobs[h].ready;
+                volatile int32_t *vs = &jobs[h].seq;
                 const unsigned long long t0 = global_ns();
-                while (*ready == 0) {  // the producer reserved this slot and is filling it
+                while (*vs != seq) {  // the producer reserved this position and is filling it
                     if (*(volatile int32_t *)&ctl->error || global_ns() - t0 > ctl->wait_limit_ns) {
-                        atomicExch(&ctl->error, 1);
+                        atomicCAS(&ctl->error, 0, 1);
                         stop = 1;
                         break;
                     }
@@ -282,12 +351,20 @@ __global__ void __launch_bounds__(HEA_BATCH_THREADS, 2)
                     job.kind = __ldcg(&src->kind);
                     job.index = __ldcg(&src->index);
                     job.iter = __ldcg(&src->iter);
+                    job.resume = __ldcg(&src->resume);
+                    job.round0 = __ldcg(&src->round0);
+                    job.miss0 = __ldcg(&src->miss0);
+                    __threadfence();
+                    if (*vs != seq) {  // reused before it was read: the ring is too small
+                        atomicCAS(&ctl->error, 0, 2);
+                        stop = 1;
+                    }
                 }
             }
         }
         __syncthreads();
         if (stop) break;
-        // this job's structure: read-only during the launch
+        // this job's structure: read-only while it is active
         const BatchStruct &d = structs[job.structure];
         {  // 8-byte words: SearchConst holds doubles, so it is 8-byte aligned and sized
             const int2 *src = reinterpret_cast<const int2 *>(&d.c);
@@ -295,40 +372,53 @@ __global__ void __launch_bounds__(HEA_BATCH_THREADS, 2)
             for (int x = threadIdx.x; x < (int)(sizeof(SearchConst) / 8); x += blockDim.x) dst[x] = __ldg(src + x);
         }
         __syncthreads();
+        unsigned long long *tally = states[job.structure].tally;
+        JobEnd e;
         switch (d.T) {
-        case 2: batch_dispatch_t<2>(c, d, job, smem, ctl->stats); break;
-        case 3: batch_dispatch_t<3>(c, d, job, smem, ctl->stats); break;
-        case 4: batch_dispatch_t<4>(c, d, job, smem, ctl->stats); break;
-        case 5: batch_dispatch_t<5>(c, d, job, smem, ctl->stats); break;
-        default: batch_dispatch_t<6>(c, d, job, smem, ctl->stats); break;
+        case 2: e = batch_dispatch_t<2>(c, d, job, smem, ctl->stats, tally, deadline); break;
+        case 3: e = batch_dispatch_t<3>(c, d, job, smem, ctl->stats, tally, deadline); break;
+        case 4: e = batch_dispatch_t<4>(c, d, job, smem, ctl->stats, tally, deadline); break;
+        case 5: e = batch_dispatch_t<5>(c, d, job, smem, ctl->stats, tally, deadline); break;
+        default: e = batch_dispatch_t<6>(c, d, job, smem, ctl->stats, tally, deadline); break;
         }
         __threadfence();  // every writer orders its results before the completion count
         __syncthreads();
         if (threadIdx.x == 0) {
-            last = atomicSub(&states[job.structure].remaining, 1) == 1;
-            if (last) {
-                __threadfence();
-                phase = __ldcg(&states[job.structure].phase);
+            if (e.yielded) {
+                enqueue_resume(jobs, ctl, d.level, job, e.round, e.miss);
+                last = 0;
+            } else {
+                last = atomicSub(&states[job.structure].remaining, 1) == 1;
+                atomicMax(&ctl->progress_ns, global_ns());
+                if (last) {
+                    __threadfence();
+                    phase = __ldcg(&states[job.structure].phase);
+                }
             }
         }
         __syncthreads();
         if (!last) continue;
         // phase transition of this structure
         const int s = job.structure, P = d.P, I = d.I, k = phase;
-        if (k == 0 && I == 0) {  // generation 0 only: the reference returns it unsorted
-            if (threadIdx.x == 0) {
-                finish_ns[s] = global_ns() - ctl->start_ns;
-                atomicAdd(&ctl->stats[3], 1ull);
-            }
-            continue;
+        bool finished = (k == 0 && I == 0);  // generation 0 only: the reference returns it unsorted
+        if (!finished) {
+            if (k > 0) block_stable_sort(d.order, d.f2, P, d.scratch);  // survivors after their search
+            if (k == I)
+                finished = true;
+            else if (k > 0 && d.tol2 >= 0.0 && __ldcg(d.f2 + __ldcg(d.order)) <= d.tol2)
+                finished = true;  // tolerance reached
+            else
+                block_stable_sort(d.order, d.f2, 2 * P, d.scratch);  // merge of iteration k
         }
-        if (k > 0) block_stable_sort(d.order, d.f2, P, d.scratch);      // survivors after their search
-        if (k < I) block_stable_sort(d.order, d.f2, 2 * P, d.scratch);  // merge of iteration k
-        if (k == I) {
+        if (finished) {
             if (threadIdx.x == 0) {
                 finish_ns[s] = global_ns() - ctl->start_ns;
+                states[s].done = 1;
+                __threadfence();
                 atomicAdd(&ctl->stats[3], 1ull);
+                atomicSub(&ctl->active, 1);
             }
+            __syncthreads();
             continue;
         }
         if (threadIdx.x == 0) {
@@ -337,8 +427,8 @@ __global__ void __launch_bounds__(HEA_BATCH_THREADS, 2)
             __threadfence();
         }
         __syncthreads();
-        enqueue_jobs(jobs, ctl, d.level, s, kJobMc2, k, P, &base);
-        if (k + 1 < I) enqueue_jobs(jobs, ctl, d.level, s, kJobGenMc, k + 1, P, &base);
+        enqueue_jobs(jobs, ctl, d.level, s, kJobMc2, k, P, &first);
+        if (k + 1 < I) enqueue_jobs(jobs, ctl, d.level, s, kJobGenMc, k + 1, P, &first);
     }
 }
 

@@ -9,7 +9,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
 #include <ctime>
+#include <deque>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -326,7 +329,7 @@ struct DeviceTables {
     }
 };
 
-int validate_problem(const hea_problem *pb)
+int validate_problem(const hea_problem *pb, bool need_nbor = true)
 {
     if (!pb) return fail(HEA_ERR_INVALID, "problem is NULL");
     if (pb->num_types < 1) return fail(HEA_ERR_INVALID, "element must name at least one species");
@@ -335,7 +338,7 @@ int validate_problem(const hea_problem *pb)
     if (pb->num_shells < 1 || pb->num_shells > kMaxShells)
         return fail(HEA_ERR_UNSUPPORTED, "number of shells (len(weight)) must be 1..%d, got %d", kMaxShells,
                     pb->num_shells);
-    if (!pb->shell_sizes || !pb->nbor || !pb->species || !pb->weight || !pb->target_sro)
+    if (!pb->shell_sizes || (need_nbor && !pb->nbor) || !pb->species || !pb->weight || !pb->target_sro)
         return fail(HEA_ERR_INVALID, "problem has a NULL array");
     int64_t n = 0;
     for (int t = 0; t < pb->num_types; ++t) {
@@ -405,17 +408,12 @@ cudaError_t allow_max_smem(F *func)
     return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_limit() - (int)a.sharedSizeBytes);
 }
 
-int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t flags = 0)
+// Search constants and padded-table geometry of a validated problem.
+void fill_const(const hea_problem *pb, uint64_t seed, SearchConst &c, PadGeom &g)
 {
-    HEA_TRY(validate_problem(pb));
     const int T = pb->num_types, S = pb->num_shells, N = pb->num_sites;
-    dt.T = T;
-    dt.S = S;
-    dt.N = N;
-    dt.ncount = (int64_t)S * T * T;
-    SearchConst &c = dt.c;
     std::memset(&c, 0, sizeof(c));
-    PadGeom g{};
+    g = PadGeom{};
     int raw_row = 0;
     for (int k = 0; k < S; ++k) raw_row += pb->shell_sizes[k];
     int off = 0, poff = 0;
@@ -455,6 +453,20 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t
                 c.R[e] = (double)N / (((double)pb->shell_sizes[k] * (double)pb->species[i]) * (double)pb->species[j]);
             }
     }
+}
+
+int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t flags = 0)
+{
+    HEA_TRY(validate_problem(pb));
+    const int T = pb->num_types, S = pb->num_shells, N = pb->num_sites;
+    dt.T = T;
+    dt.S = S;
+    dt.N = N;
+    dt.ncount = (int64_t)S * T * T;
+    SearchConst &c = dt.c;
+    PadGeom g;
+    fill_const(pb, seed, c, g);
+    const int raw_row = g.raw_row, poff = g.pad_row;
 
     // shared memory of the two kernels
     const size_t cnt_bytes = 4 * (size_t)((dt.ncount + 3) & ~3);
@@ -1228,17 +1240,21 @@ __global__ void batch_reset_kernel(BatchCtl *ctl, BatchJob *jobs, unsigned long 
 {
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < njobs;
          i += (unsigned long long)gridDim.x * blockDim.x)
-        jobs[i].ready = 0;
+        jobs[i].seq = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         for (int l = 0; l < kBatchLevels; ++l) {
             ctl->q[l].head = 0;
             ctl->q[l].tail = 0;
-            ctl->q[l].total = lv.total[l];
+            ctl->q[l].cap = lv.total[l] ? lv.total[l] : 1;
             ctl->q[l].base = lv.base[l];
         }
         for (int i = 0; i < 4; ++i) ctl->stats[i] = 0;
         ctl->error = 0;
+        ctl->active = 0;
         ctl->wait_limit_ns = limit_ns;
+        ctl->start_ns = global_ns();
+        ctl->progress_ns = ctl->start_ns;
+        ctl->deadline_ns = 0;
     }
 }
 
@@ -1257,6 +1273,29 @@ int batch_layout(const SearchConst &c, int S)
     if (S == 3 && c.chunks[0] == 2 && c.chunks[1] == 2 && c.chunks[2] == 3) return kLayBcc;
     if (S == 3 && c.chunks[0] == 3 && c.chunks[1] == 2 && c.chunks[2] == 6) return kLayFccTrue;
     return S == 1 ? kLayRt1 : (S == 2 ? kLayRt2 : kLayRt3);
+}
+
+// Shared memory of one batch job: occupancy (unless it stays in HBM), per-warp
+// counts and the double-buffered swap records.
+size_t batch_job_smem(int occ_stride, int64_t ncount, int nwarps, bool hbm)
+{
+    return (hbm ? 0 : (size_t)occ_stride + 16) + (size_t)nwarps * (4 * mc_ncount_pad((int)ncount) + 2 * sizeof(SwapRecord));
+}
+
+// Dynamic shared memory per CTA that still lets two batch CTAs share an SM.
+int batch_smem_budget(size_t *out)
+{
+    cudaFuncAttributes a;
+    int dev = 0, per_sm = 0, reserved = 0;
+    HEA_CUDA(cudaFuncGetAttributes(&a, batch_kernel));
+    HEA_CUDA(cudaGetDevice(&dev));
+    HEA_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    HEA_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    long long b = (long long)per_sm / 2 - reserved - (long long)a.sharedSizeBytes;
+    b &= ~127ll;
+    const long long lim = (long long)smem_limit() - (long long)a.sharedSizeBytes;
+    *out = (size_t)std::max(0ll, std::min(b, lim));
+    return HEA_OK;
 }
 
 }  // namespace
@@ -1297,6 +1336,7 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
         d.D = params[i].converge_depth;
         d.I = params[i].total_iter;
         d.max_rounds = params[i].max_rounds > 0 ? params[i].max_rounds : (int64_t)1 << 31;
+        d.tol2 = -1.0;
         d.T = t->T;
         d.layout = batch_layout(t->c, t->S);
         if ((rc = batch_alloc(b, &d.occ, (size_t)slots * t->c.occ_stride)) != HEA_OK) break;
@@ -1310,8 +1350,15 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
         }
         b->h_structs.push_back(d);
         b->total_jobs += d.I > 0 ? (unsigned long long)P * (2 * d.I + 1) : (unsigned long long)P;
-        const size_t sm = mc_smem(t->c.occ_stride, (int)t->ncount, nwarps);
-        if (sm > b->smem) b->smem = sm;
+    }
+    // occupancy in shared memory when two CTAs per SM still fit, else in HBM
+    size_t budget = 0;
+    if (rc == HEA_OK) rc = batch_smem_budget(&budget);
+    for (int i = 0; rc == HEA_OK && i < count; ++i) {
+        BatchStruct &d = b->h_structs[i];
+        const int64_t ncount = b->tables[i]->ncount;
+        d.hbm = batch_job_smem(d.c.occ_stride, ncount, nwarps, false) > budget ? 1 : 0;
+        b->smem = std::max(b->smem, batch_job_smem(d.c.occ_stride, ncount, nwarps, d.hbm != 0));
     }
     // priority levels: structures ranked by work, largest first
     BatchLevels lv{};
@@ -1368,7 +1415,7 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
         if (e == cudaSuccess) e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             batch_reset_kernel<<<64, 256, 0, b->stream>>>(b->d_ctl, b->d_jobs, b->total_jobs, lv, 60ull * 1000000000ull);
-            batch_seed_kernel<<<count, 256, 0, b->stream>>>(b->d_structs, b->d_states, b->d_jobs, b->d_ctl);
+            batch_seed_kernel<<<count, 256, 0, b->stream>>>(b->d_structs, nullptr, b->d_states, b->d_jobs, b->d_ctl);
             batch_kernel<<<b->grid, b->block, b->smem, b->stream>>>(b->d_structs, b->d_states, b->d_jobs, b->d_ctl,
                                                                     b->d_finish);
             cudaError_t e2 = cudaStreamEndCapture(b->stream, &b->graph);
@@ -1403,7 +1450,9 @@ int hea_batch_run(hea_batch *b, const uint64_t *seeds, hea_stats *stats)
     BatchCtl ctl;
     HEA_CUDA(cudaMemcpy(&ctl, b->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
     if (ctl.error)
-        return fail(HEA_ERR_CUDA, "batched search stopped: a wait for queued work exceeded its time limit");
+        return fail(HEA_ERR_CUDA, "batched search stopped: %s",
+                    ctl.error == 2 ? "a job-ring slot was reused before it was read"
+                                   : "a wait for queued work exceeded its time limit");
     if (ctl.stats[3] != (unsigned long long)b->count)
         return fail(HEA_ERR_CUDA, "batched search finished %llu of %d structures", ctl.stats[3], b->count);
     if (stats) {
@@ -1447,5 +1496,673 @@ int hea_batch_finish_times(hea_batch *b, double *out_ms)
 }
 
 void hea_batch_destroy(hea_batch *b) { delete b; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Serving loop (hea_server_*): the job engine of hea_batch.cuh run in time
+// slices.  Between slices the host admits queued requests (tables built or
+// uploaded into a device arena, phase-0 jobs seeded) and collects finished
+// ones; requests still running keep their state on the device.
+// ---------------------------------------------------------------------------
+namespace {
+
+using ServerClock = std::chrono::steady_clock;
+
+// First-fit sub-allocation of one device buffer in 256-byte granules.
+struct ArenaHeap {
+    std::map<size_t, size_t> free_;  // offset -> bytes
+    size_t total = 0, free_bytes = 0;
+    static size_t round(size_t b) { return (b + 255) & ~(size_t)255; }
+    void init(size_t bytes)
+    {
+        total = free_bytes = bytes & ~(size_t)255;
+        free_.clear();
+        if (total) free_[0] = total;
+    }
+    bool alloc(size_t bytes, size_t *off)
+    {
+        bytes = round(bytes);
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            *off = it->first;
+            const size_t rest = it->second - bytes, next = it->first + bytes;
+            free_.erase(it);
+            if (rest) free_[next] = rest;
+            free_bytes -= bytes;
+            return true;
+        }
+        return false;
+    }
+    void release(size_t off, size_t bytes)
+    {
+        bytes = round(bytes);
+        free_bytes += bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+};
+
+struct ServerRequest {
+    int64_t id = 0;
+    int state = 0;  // 0 queued, 1 on the device, 2 finished, 3 failed
+    hea_params params{};
+    double tol2 = -1.0;
+    int level = 0;
+    int N = 0, T = 0, S = 0;
+    std::vector<int32_t> shell_sizes, species, nbor;  // nbor empty for lattice requests
+    std::vector<double> weight, target;
+    int lattice = -1, cell = 0, shell_set = 0;
+    int slot = -1, hbm = 0;
+    size_t off = 0, bytes = 0;
+    double t_submit = 0, t_admit = 0, t_finish = 0, device_ms = 0;
+    int iterations = 0;
+    unsigned long long tally[3] = {0, 0, 0};
+    std::vector<uint8_t> occ;
+    std::vector<double> fit;
+    std::string error;
+
+    hea_problem problem() const
+    {
+        hea_problem p{};
+        p.num_sites = N;
+        p.num_types = T;
+        p.num_shells = S;
+        p.shell_sizes = const_cast<int32_t *>(shell_sizes.data());
+        p.nbor = nbor.empty() ? nullptr : const_cast<int32_t *>(nbor.data());
+        p.species = const_cast<int32_t *>(species.data());
+        p.weight = const_cast<double *>(weight.data());
+        p.target_sro = const_cast<double *>(target.data());
+        return p;
+    }
+};
+
+// Arena bytes of a request: padded table, then 2P occupancy rows, counts,
+// f2, order and sort scratch, each 256-byte aligned.
+struct RequestLayout {
+    size_t nbor, occ, cnt, f2, order, scratch, total;
+};
+
+RequestLayout request_layout(const SearchConst &c, int64_t pad_row, int S, int T, int P)
+{
+    RequestLayout L{};
+    const size_t slots = 2 * (size_t)P;
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = o;
+        o += ArenaHeap::round(bytes);
+        return at;
+    };
+    L.nbor = take((size_t)c.num_sites * pad_row * sizeof(int32_t));
+    L.occ = take(slots * c.occ_stride);
+    L.cnt = take(slots * (size_t)S * T * T * sizeof(int32_t));
+    L.f2 = take(slots * sizeof(double));
+    L.order = take(slots * sizeof(int32_t));
+    L.scratch = take(slots * sizeof(int32_t));
+    L.total = o;
+    return L;
+}
+
+__global__ void server_arm_kernel(BatchCtl *ctl, unsigned long long slice_ns)
+{
+    const unsigned long long now = global_ns();
+    ctl->deadline_ns = now + slice_ns;
+    ctl->progress_ns = now;
+}
+
+}  // namespace
+
+struct hea_server {
+    hea_server_config cfg{};
+    int nwarps = HEA_BATCH_THREADS / 32;
+    int grid = 0;
+    size_t smem = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<void *> buffers;
+    uint8_t *arena = nullptr;
+    ArenaHeap heap;
+    BatchStruct *d_structs = nullptr;
+    BatchState *d_states = nullptr;
+    BatchJob *d_jobs = nullptr;
+    BatchCtl *d_ctl = nullptr;
+    unsigned long long *d_finish = nullptr;
+    int32_t *d_list = nullptr;
+    int *d_err = nullptr;  // per slot: table check flags
+    void *d_raw = nullptr;
+    size_t raw_bytes = 0;
+    void *d_out = nullptr;
+    size_t out_bytes = 0;
+    double *d_out_f2 = nullptr;
+    std::vector<BatchStruct> h_structs;
+    std::vector<BatchState> h_states;
+    std::vector<unsigned long long> h_finish;
+    std::vector<int> h_err;
+    std::vector<int32_t> h_list;
+    std::vector<int64_t> slot_req;                // request id per slot, 0 = free
+    unsigned long long level_load[kBatchLevels] = {};  // ring slots held per level
+    std::map<int64_t, ServerRequest> reqs;
+    std::deque<int64_t> queue;
+    int64_t next_id = 1;
+    ServerClock::time_point t0;
+    double busy_ms = 0;
+    int launches = 0;
+    int running = 0;
+    unsigned long long finished_total = 0;
+    BatchCtl last_ctl{};
+    std::string broken;  // set after a device-side failure; every later call fails with it
+
+    ~hea_server()
+    {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void *p : buffers) cudaFree(p);
+        if (d_raw) cudaFree(d_raw);
+        if (d_out) cudaFree(d_out);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    double now_ms() const
+    {
+        return std::chrono::duration<double, std::milli>(ServerClock::now() - t0).count();
+    }
+    template <class X>
+    int alloc(X **p, size_t bytes)
+    {
+        void *q = nullptr;
+        if (cudaMalloc(&q, bytes) != cudaSuccess) return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes", bytes);
+        buffers.push_back(q);
+        *p = static_cast<X *>(q);
+        return HEA_OK;
+    }
+    // grow a scratch buffer between slices (nothing of this server is running)
+    int grow(void **p, size_t *have, size_t need)
+    {
+        if (need <= *have) return HEA_OK;
+        HEA_CUDA(cudaStreamSynchronize(stream));
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        *have = 0;
+        if (cudaMalloc(p, need) != cudaSuccess) return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes", need);
+        *have = need;
+        return HEA_OK;
+    }
+};
+
+namespace {
+
+int server_broken(hea_server *sv) { return fail(HEA_ERR_CUDA, "server stopped: %s", sv->broken.c_str()); }
+
+// Arena layout, table preparation and structure entry of one request in
+// `slot`.  Returns HEA_OK, or HEA_PENDING when memory or ring room is short
+// (the request stays queued).
+int server_place(hea_server *sv, ServerRequest &r, int slot)
+{
+    const hea_problem pb = r.problem();
+    SearchConst c;
+    PadGeom g;
+    fill_const(&pb, r.params.seed, c, g);
+    int raw_row = g.raw_row;
+    LatticeSpec sp{};
+    if (r.lattice >= 0) {
+        HEA_TRY(make_lattice_spec(r.lattice, r.shell_set, sp));
+        raw_row = sp.size[0] + sp.size[1] + sp.size[2];
+    }
+    const int P = r.params.num_solutions;
+    const RequestLayout L = request_layout(c, g.pad_row, r.S, r.T, P);
+    if (sv->level_load[r.level] + 2ull * P > (unsigned long long)sv->cfg.ring_jobs) return HEA_PENDING;
+    size_t off = 0;
+    if (!sv->heap.alloc(L.total, &off)) return HEA_PENDING;
+    r.off = off;
+    r.bytes = L.total;
+    uint8_t *base = sv->arena + off;
+
+    // raw table (uploaded or built), then its padded, checked copy
+    const size_t raw = (size_t)r.N * raw_row * sizeof(int32_t);
+    int rc = sv->grow(&sv->d_raw, &sv->raw_bytes, raw);
+    if (rc != HEA_OK) {
+        sv->heap.release(off, L.total);
+        return rc;
+    }
+    cudaError_t e = cudaMemsetAsync(sv->d_err + slot, 0, sizeof(int), sv->stream);
+    if (e == cudaSuccess) {
+        if (r.lattice >= 0) {
+            const int blocks = (int)std::min<int64_t>(((int64_t)r.N + 255) / 256, 4096);
+            build_neighbors_kernel<<<blocks, 256, 0, sv->stream>>>(sp, r.cell, (int32_t *)sv->d_raw, raw_row,
+                                                                    sv->d_err + slot);
+            e = cudaGetLastError();
+        } else {
+            e = cudaMemcpyAsync(sv->d_raw, r.nbor.data(), raw, cudaMemcpyHostToDevice, sv->stream);
+        }
+    }
+    g.raw_row = raw_row;
+    if (e == cudaSuccess) {
+        pad_and_check_kernel<<<1184, 256, 0, sv->stream>>>((const int32_t *)sv->d_raw, (int32_t *)(base + L.nbor), g,
+                                                            sv->d_err + slot);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(base + L.occ, 0, L.cnt - L.occ, sv->stream);
+    if (e != cudaSuccess) {
+        sv->heap.release(off, L.total);
+        return fail(HEA_ERR_CUDA, "request set-up failed: %s", cudaGetErrorString(e));
+    }
+    BatchStruct d{};
+    d.c = c;
+    d.nbor = reinterpret_cast<const int4 *>(base + L.nbor);
+    d.occ = base + L.occ;
+    d.cnt = reinterpret_cast<int32_t *>(base + L.cnt);
+    d.f2 = reinterpret_cast<double *>(base + L.f2);
+    d.order = reinterpret_cast<int32_t *>(base + L.order);
+    d.scratch = reinterpret_cast<int32_t *>(base + L.scratch);
+    d.P = P;
+    d.Q = r.params.parallel_task;
+    d.D = r.params.converge_depth;
+    d.I = r.params.total_iter;
+    d.max_rounds = r.params.max_rounds > 0 ? r.params.max_rounds : (int64_t)1 << 31;
+    d.tol2 = r.tol2;
+    d.T = r.T;
+    d.layout = batch_layout(c, r.S);
+    d.level = r.level;
+    d.hbm = (batch_job_smem(c.occ_stride, (int64_t)r.S * r.T * r.T, sv->nwarps, false) > sv->smem ||
+             (sv->cfg.hbm_sites > 0 && r.N >= sv->cfg.hbm_sites))
+                ? 1
+                : 0;
+    r.hbm = d.hbm;
+    sv->h_structs[slot] = d;
+    sv->level_load[r.level] += 2ull * P;
+    r.slot = slot;
+    return HEA_OK;
+}
+
+void server_release(hea_server *sv, ServerRequest &r)
+{
+    if (r.slot < 0) return;
+    sv->heap.release(r.off, r.bytes);
+    sv->level_load[r.level] -= 2ull * r.params.num_solutions;
+    sv->slot_req[r.slot] = 0;
+    r.slot = -1;
+}
+
+// Admit queued requests in submission order while slots, arena memory and
+// ring room allow; seed their phase-0 jobs.
+int server_admit(hea_server *sv)
+{
+    std::vector<int64_t> placed;
+    while (!sv->queue.empty()) {
+        int slot = -1;
+        for (int i = 0; i < sv->cfg.max_requests; ++i)
+            if (sv->slot_req[i] == 0) {
+                slot = i;
+                break;
+            }
+        if (slot < 0) break;
+        ServerRequest &r = sv->reqs[sv->queue.front()];
+        const int rc = server_place(sv, r, slot);
+        if (rc == HEA_PENDING) break;
+        if (rc != HEA_OK) return rc;
+        sv->slot_req[slot] = r.id;
+        placed.push_back(r.id);
+        sv->queue.pop_front();
+    }
+    if (placed.empty()) return HEA_OK;
+    // table checks of the placed requests
+    HEA_CUDA(cudaMemcpyAsync(sv->h_err.data(), sv->d_err, sizeof(int) * sv->cfg.max_requests, cudaMemcpyDeviceToHost,
+                             sv->stream));
+    HEA_CUDA(cudaStreamSynchronize(sv->stream));
+    sv->h_list.clear();
+    const double t = sv->now_ms();
+    for (int64_t id : placed) {
+        ServerRequest &r = sv->reqs[id];
+        const int err = sv->h_err[r.slot];
+        if (err) {
+            r.state = 3;
+            r.error = (err & 1) ? "neighbour list holds an id outside the structure"
+                      : (err & 2) ? "neighbour list names a site as its own neighbour"
+                                  : "neighbour list is not symmetric within a shell";
+            r.t_finish = t;
+            server_release(sv, r);
+            continue;
+        }
+        r.state = 1;
+        r.t_admit = t;
+        sv->h_list.push_back(r.slot);
+        HEA_CUDA(cudaMemcpyAsync(sv->d_structs + r.slot, &sv->h_structs[r.slot], sizeof(BatchStruct),
+                                 cudaMemcpyHostToDevice, sv->stream));
+        ++sv->running;
+    }
+    if (sv->h_list.empty()) return HEA_OK;
+    HEA_CUDA(cudaMemcpyAsync(sv->d_list, sv->h_list.data(), sizeof(int32_t) * sv->h_list.size(),
+                             cudaMemcpyHostToDevice, sv->stream));
+    batch_seed_kernel<<<(unsigned)sv->h_list.size(), 256, 0, sv->stream>>>(sv->d_structs, sv->d_list, sv->d_states,
+                                                                             sv->d_jobs, sv->d_ctl);
+    HEA_CUDA(cudaGetLastError());
+    return HEA_OK;
+}
+
+// Results of the requests that finished in the last slice.
+int server_collect(hea_server *sv, int32_t *finished)
+{
+    const double t = sv->now_ms();
+    for (int slot = 0; slot < sv->cfg.max_requests; ++slot) {
+        const int64_t id = sv->slot_req[slot];
+        if (!id || !sv->h_states[slot].done) continue;
+        ServerRequest &r = sv->reqs[id];
+        if (r.state != 1) continue;
+        const BatchStruct &d = sv->h_structs[slot];
+        const size_t rows = (size_t)d.P * d.c.num_sites;
+        HEA_TRY(sv->grow(&sv->d_out, &sv->out_bytes, rows));
+        dim3 grid((unsigned)std::min(64, (d.c.num_sites + 255) / 256), (unsigned)d.P);
+        gather_rows_kernel<<<grid, 256, 0, sv->stream>>>(d.occ, d.order, d.P, d.c.occ_stride, d.c.num_sites, d.f2,
+                                                        (uint8_t *)sv->d_out, sv->d_out_f2);
+        HEA_CUDA(cudaGetLastError());
+        r.occ.resize(rows);
+        r.fit.resize(d.P);
+        HEA_CUDA(cudaMemcpyAsync(r.occ.data(), sv->d_out, rows, cudaMemcpyDeviceToHost, sv->stream));
+        HEA_CUDA(cudaMemcpyAsync(r.fit.data(), sv->d_out_f2, d.P * sizeof(double), cudaMemcpyDeviceToHost, sv->stream));
+        HEA_CUDA(cudaStreamSynchronize(sv->stream));
+        for (double &f : r.fit) f = std::sqrt(f);
+        r.state = 2;
+        r.t_finish = t;
+        r.device_ms = sv->h_finish[slot] * 1e-6;
+        r.iterations = sv->h_states[slot].phase;
+        for (int k = 0; k < 3; ++k) r.tally[k] = sv->h_states[slot].tally[k];
+        server_release(sv, r);
+        --sv->running;
+        ++sv->finished_total;
+        ++*finished;
+    }
+    return HEA_OK;
+}
+
+void fill_info(const ServerRequest &r, hea_request_info *info)
+{
+    if (!info) return;
+    std::memset(info, 0, sizeof(*info));
+    info->state = r.state;
+    info->iterations = r.iterations;
+    info->hbm = r.hbm;
+    info->submit_ms = r.t_submit;
+    info->admit_ms = r.t_admit;
+    info->finish_ms = r.t_finish;
+    info->device_ms = r.device_ms;
+    info->rounds = (int64_t)r.tally[0];
+    info->evals = (int64_t)r.tally[1];
+    info->accepts = (int64_t)r.tally[2];
+    info->device_bytes = (int64_t)r.bytes;
+}
+
+int server_enqueue(hea_server *sv, ServerRequest &&r, const hea_params *params, double tolerance, int32_t priority,
+                   int64_t *out_id)
+{
+    HEA_TRY(validate_params(params));
+    if (std::isnan(tolerance) || tolerance == INFINITY) return fail(HEA_ERR_INVALID, "tolerance must be finite");
+    if (priority < 0 || priority >= kBatchLevels)
+        return fail(HEA_ERR_INVALID, "priority must be 0..%d, got %d", kBatchLevels - 1, priority);
+    if (params->max_rounds > ((int64_t)1 << 31))
+        return fail(HEA_ERR_INVALID, "max_rounds above 2^31 is not supported by the server");
+    if (2ll * params->num_solutions > sv->cfg.ring_jobs)
+        return fail(HEA_ERR_UNSUPPORTED, "2 * nnet = %d exceeds the job ring (%d)", 2 * params->num_solutions,
+                    sv->cfg.ring_jobs);
+    r.params = *params;
+    r.tol2 = tolerance >= 0 ? tolerance * tolerance : -1.0;
+    r.level = priority;
+    {  // memory the request will need must fit the arena at all
+        const hea_problem pb = r.problem();
+        SearchConst c;
+        PadGeom g;
+        fill_const(&pb, params->seed, c, g);
+        const RequestLayout L = request_layout(c, g.pad_row, r.S, r.T, params->num_solutions);
+        if (L.total > sv->heap.total)
+            return fail(HEA_ERR_UNSUPPORTED, "request needs %zu bytes of device memory; the arena holds %zu", L.total,
+                        sv->heap.total);
+    }
+    r.id = sv->next_id++;
+    r.state = 0;
+    r.t_submit = sv->now_ms();
+    const int64_t id = r.id;
+    sv->reqs.emplace(id, std::move(r));
+    sv->queue.push_back(id);
+    if (out_id) *out_id = id;
+    return HEA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hea_server_create(const hea_server_config *config, hea_server **out)
+{
+    if (!out) return fail(HEA_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    hea_server_config cfg{};
+    if (config) cfg = *config;
+    if (cfg.max_requests <= 0) cfg.max_requests = 256;
+    if (cfg.ring_jobs <= 0) cfg.ring_jobs = 65536;
+    if (cfg.slice_ms <= 0) cfg.slice_ms = 10.0;
+    if (cfg.max_requests > 65536) return fail(HEA_ERR_INVALID, "max_requests must be <= 65536");
+    if (cfg.ring_jobs > (1 << 26)) return fail(HEA_ERR_INVALID, "ring_jobs must be <= 2^26");
+    hea_server *sv = new (std::nothrow) hea_server();
+    if (!sv) return fail(HEA_ERR_NOMEM, "out of host memory");
+    sv->t0 = ServerClock::now();
+    int rc = HEA_OK;
+    if (cfg.arena_bytes <= 0) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) rc = fail(HEA_ERR_CUDA, "cannot query device memory");
+        cfg.arena_bytes = (int64_t)std::min(fr / 2, (size_t)8 << 30);
+    }
+    size_t budget = 0;
+    if (rc == HEA_OK) rc = batch_smem_budget(&budget);
+    if (rc == HEA_OK) {
+        const size_t least = batch_job_smem(0, (int64_t)kMaxShells * kMaxTypes * kMaxTypes, sv->nwarps, true);
+        sv->smem = cfg.smem_bytes > 0 ? (size_t)cfg.smem_bytes : budget;
+        sv->smem = std::max(sv->smem, least);
+        cudaFuncAttributes a;
+        if (cudaFuncGetAttributes(&a, batch_kernel) != cudaSuccess) rc = fail(HEA_ERR_CUDA, "cannot query the batch kernel");
+        else if (sv->smem + a.sharedSizeBytes > (size_t)smem_limit())
+            rc = fail(HEA_ERR_INVALID, "smem_bytes %zu above the device limit", sv->smem);
+        cfg.smem_bytes = (int32_t)sv->smem;
+    }
+    sv->cfg = cfg;
+    const int M = cfg.max_requests;
+    if (rc == HEA_OK) rc = sv->alloc(&sv->arena, (size_t)cfg.arena_bytes);
+    if (rc == HEA_OK) rc = sv->alloc(&sv->d_structs, sizeof(BatchStruct) * M);
+    if (rc == HEA_OK) rc = sv->alloc(&sv->d_states, sizeof(BatchState) * M);
+    if (rc == HEA_OK) rc = sv->alloc(&sv->d_jobs, sizeof(BatchJob) * (size_t)cfg.ring_jobs * kBatchLevels);
+    if (rc == HEA_OK) rc = sv->alloc(&sv->d_ctl, sizeof(BatchCtl));
+    if (rc == HEA_OK) rc = sv->alloc(&sv->d_finish, sizeof(unsigned long long) * M);
+    if (rc == HEA_OK) rc = sv->alloc(&sv->d_list, sizeof(int32_t) * M);
+    if (rc == HEA_OK) rc = sv->alloc(&sv->d_err, sizeof(int) * M);
+    if (rc == HEA_OK) rc = sv->alloc(&sv->d_out_f2, sizeof(double) * 65536);
+    if (rc == HEA_OK) {
+        sv->heap.init((size_t)cfg.arena_bytes);
+        sv->h_structs.assign(M, BatchStruct{});
+        sv->h_states.assign(M, BatchState{});
+        sv->h_finish.assign(M, 0);
+        sv->h_err.assign(M, 0);
+        sv->slot_req.assign(M, 0);
+        sv->h_list.reserve(M);
+        cudaError_t e = allow_max_smem(batch_kernel);
+        int per_sm = 0, sms = 0, dev = 0;
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, HEA_BATCH_THREADS, sv->smem);
+        if (e == cudaSuccess) e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreate(&sv->ev0);
+        if (e == cudaSuccess) e = cudaEventCreate(&sv->ev1);
+        if (e == cudaSuccess) e = cudaMemsetAsync(sv->d_states, 0, sizeof(BatchState) * M, sv->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(sv->d_finish, 0, sizeof(unsigned long long) * M, sv->stream);
+        if (e == cudaSuccess) {
+            BatchLevels lv{};
+            for (int l = 0; l < kBatchLevels; ++l) {
+                lv.total[l] = (unsigned long long)cfg.ring_jobs;
+                lv.base[l] = (unsigned long long)l * cfg.ring_jobs;
+            }
+            batch_reset_kernel<<<64, 256, 0, sv->stream>>>(sv->d_ctl, sv->d_jobs,
+                                                          (unsigned long long)cfg.ring_jobs * kBatchLevels, lv,
+                                                          10ull * 1000000000ull);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(sv->stream);
+        if (e != cudaSuccess) rc = fail(HEA_ERR_CUDA, "server set-up failed: %s", cudaGetErrorString(e));
+        else if (per_sm < 1) rc = fail(HEA_ERR_UNSUPPORTED, "batch kernel does not fit on an SM");
+        sv->grid = per_sm * sms;
+    }
+    if (rc != HEA_OK) {
+        delete sv;
+        return rc;
+    }
+    *out = sv;
+    return HEA_OK;
+}
+
+int hea_server_submit(hea_server *server, const hea_problem *problem, const hea_params *params, double tolerance,
+                      int32_t priority, int64_t *out_id)
+{
+    if (!server) return fail(HEA_ERR_INVALID, "server is NULL");
+    if (!server->broken.empty()) return server_broken(server);
+    HEA_TRY(validate_problem(problem));
+    ServerRequest r;
+    r.N = problem->num_sites;
+    r.T = problem->num_types;
+    r.S = problem->num_shells;
+    r.shell_sizes.assign(problem->shell_sizes, problem->shell_sizes + r.S);
+    r.species.assign(problem->species, problem->species + r.T);
+    r.weight.assign(problem->weight, problem->weight + r.S);
+    r.target.assign(problem->target_sro, problem->target_sro + (size_t)r.S * r.T * r.T);
+    int64_t row = 0;
+    for (int k = 0; k < r.S; ++k) row += r.shell_sizes[k];
+    r.nbor.assign(problem->nbor, problem->nbor + (size_t)r.N * row);
+    return server_enqueue(server, std::move(r), params, tolerance, priority, out_id);
+}
+
+int hea_server_submit_lattice(hea_server *server, int32_t lattice, int32_t cell, int32_t shell_set,
+                              int32_t num_types, int32_t num_shells, const int32_t *species, const double *weight,
+                              const double *target_sro, const hea_params *params, double tolerance,
+                              int32_t priority, int64_t *out_id)
+{
+    if (!server) return fail(HEA_ERR_INVALID, "server is NULL");
+    if (!server->broken.empty()) return server_broken(server);
+    int32_t sizes[3] = {0, 0, 0}, n = 0;
+    HEA_TRY(hea_build_neighbors(lattice, cell, shell_set, nullptr, sizes, &n));
+    if (num_shells < 1 || num_shells > 3) return fail(HEA_ERR_UNSUPPORTED, "num_shells must be 1..3, got %d", num_shells);
+    if (!species || !weight || !target_sro) return fail(HEA_ERR_INVALID, "species, weight and target_sro are required");
+    ServerRequest r;
+    r.N = n;
+    r.T = num_types;
+    r.S = num_shells;
+    r.shell_sizes.assign(sizes, sizes + num_shells);
+    if (num_types < 1 || num_types > kMaxTypes)
+        return fail(HEA_ERR_UNSUPPORTED, "number of species must be 2..%d, got %d", kMaxTypes, num_types);
+    r.species.assign(species, species + num_types);
+    r.weight.assign(weight, weight + num_shells);
+    r.target.assign(target_sro, target_sro + (size_t)num_shells * num_types * num_types);
+    r.lattice = lattice;
+    r.cell = cell;
+    r.shell_set = shell_set;
+    const hea_problem pb = r.problem();
+    HEA_TRY(validate_problem(&pb, false));
+    return server_enqueue(server, std::move(r), params, tolerance, priority, out_id);
+}
+
+int hea_server_step(hea_server *server, int32_t *out_finished)
+{
+    if (!server) return fail(HEA_ERR_INVALID, "server is NULL");
+    if (out_finished) *out_finished = 0;
+    hea_server *sv = server;
+    if (!sv->broken.empty()) return server_broken(sv);
+    HEA_TRY(server_admit(sv));
+    if (sv->running == 0) return HEA_OK;
+    const int M = sv->cfg.max_requests;
+    HEA_CUDA(cudaEventRecord(sv->ev0, sv->stream));
+    server_arm_kernel<<<1, 1, 0, sv->stream>>>(sv->d_ctl, (unsigned long long)(sv->cfg.slice_ms * 1e6));
+    batch_kernel<<<sv->grid, HEA_BATCH_THREADS, sv->smem, sv->stream>>>(sv->d_structs, sv->d_states, sv->d_jobs,
+                                                                         sv->d_ctl, sv->d_finish);
+    HEA_CUDA(cudaGetLastError());
+    HEA_CUDA(cudaEventRecord(sv->ev1, sv->stream));
+    HEA_CUDA(cudaMemcpyAsync(&sv->last_ctl, sv->d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, sv->stream));
+    HEA_CUDA(cudaMemcpyAsync(sv->h_states.data(), sv->d_states, sizeof(BatchState) * M, cudaMemcpyDeviceToHost,
+                             sv->stream));
+    HEA_CUDA(cudaMemcpyAsync(sv->h_finish.data(), sv->d_finish, sizeof(unsigned long long) * M,
+                             cudaMemcpyDeviceToHost, sv->stream));
+    HEA_CUDA(cudaStreamSynchronize(sv->stream));
+    float ms = 0;
+    HEA_CUDA(cudaEventElapsedTime(&ms, sv->ev0, sv->ev1));
+    sv->busy_ms += ms;
+    ++sv->launches;
+    if (sv->last_ctl.error) {
+        sv->broken = sv->last_ctl.error == 2 ? "a job-ring slot was reused before it was read"
+                                             : "a wait for queued work exceeded its time limit";
+        return server_broken(sv);
+    }
+    int32_t fin = 0;
+    HEA_TRY(server_collect(sv, &fin));
+    if (out_finished) *out_finished = fin;
+    return HEA_OK;
+}
+
+int hea_server_info(hea_server *server, int64_t id, hea_request_info *info)
+{
+    if (!server) return fail(HEA_ERR_INVALID, "server is NULL");
+    auto it = server->reqs.find(id);
+    if (it == server->reqs.end()) return fail(HEA_ERR_INVALID, "no request %lld", (long long)id);
+    fill_info(it->second, info);
+    return HEA_OK;
+}
+
+int hea_server_result(hea_server *server, int64_t id, uint8_t *out_occ, double *out_fitness, hea_request_info *info)
+{
+    if (!server) return fail(HEA_ERR_INVALID, "server is NULL");
+    auto it = server->reqs.find(id);
+    if (it == server->reqs.end()) return fail(HEA_ERR_INVALID, "no request %lld", (long long)id);
+    ServerRequest &r = it->second;
+    fill_info(r, info);
+    if (r.state == 0 || r.state == 1) return HEA_PENDING;
+    if (r.state == 3) {
+        const std::string m = r.error;
+        server->reqs.erase(it);
+        return fail(HEA_ERR_UNSUPPORTED, "request %lld failed: %s", (long long)id, m.c_str());
+    }
+    if (out_occ) std::memcpy(out_occ, r.occ.data(), r.occ.size());
+    if (out_fitness) std::memcpy(out_fitness, r.fit.data(), r.fit.size() * sizeof(double));
+    server->reqs.erase(it);
+    return HEA_OK;
+}
+
+int hea_server_status_get(hea_server *server, hea_server_status *status)
+{
+    if (!server || !status) return fail(HEA_ERR_INVALID, "server and status must not be NULL");
+    std::memset(status, 0, sizeof(*status));
+    int unread = 0, free_slots = 0;
+    for (const auto &kv : server->reqs) unread += (kv.second.state == 2 || kv.second.state == 3);
+    for (int64_t s : server->slot_req) free_slots += (s == 0);
+    status->queued = (int32_t)server->queue.size();
+    status->running = server->running;
+    status->finished_unread = unread;
+    status->slots_free = free_slots;
+    status->arena_free_bytes = (int64_t)server->heap.free_bytes;
+    status->arena_bytes = (int64_t)server->heap.total;
+    status->rounds = (int64_t)server->last_ctl.stats[0];
+    status->evals = (int64_t)server->last_ctl.stats[1];
+    status->accepts = (int64_t)server->last_ctl.stats[2];
+    status->finished = (int64_t)server->finished_total;
+    status->busy_ms = server->busy_ms;
+    status->launches = server->launches;
+    status->smem_bytes = (int32_t)server->smem;
+    return HEA_OK;
+}
+
+void hea_server_destroy(hea_server *server) { delete server; }
 
 }  // extern "C"

@@ -81,4 +81,12 @@ inline int feistel_half_bits(uint32_t n)
     return (b + 1) / 2;
 }
 
+// Device wall clock in nanoseconds (the %globaltimer register).
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 }  // namespace hea

@@ -448,23 +448,40 @@ struct McTrace {
 
 struct McTally {
     double f2;
-    int64_t rounds, accepts, evals;
+    int64_t rounds, accepts, evals;  // rounds run by this call
+    int64_t round_end;               // round index the search continues from
+    int miss;                        // consecutive rejections at round_end
+    bool yielded;                    // stopped at the deadline before converging
+};
+
+// Where a search segment starts: a search stopped at a round boundary
+// continues from (round0, miss0) with the same occupancy, counts and f2 and
+// draws the same proposals as one that never stopped.
+struct McResume {
+    int64_t round0;
+    int miss0;
+    unsigned long long deadline_ns;  // kYield: stop after the first round ending past this device time (0: never)
+    double tol2;                     // kYield: the search ends once f2 <= tol2 (< 0: never)
 };
 
 // Rounds of the local search on the staged state (occ5, the per-warp count
 // copies in cnt_all).  Every thread returns the same f2/rounds/accepts; evals
-// is this thread's count.  No barrier at entry; one per round.
-template <int T, class L, bool kAhead = false>
+// is this thread's count.  No barrier at entry; one per round.  occ5 may be
+// shared or global memory; every thread writes the accepted swap's bytes
+// itself, so its own later loads see them either way.
+template <int T, class L, bool kAhead = false, bool kYield = false>
 __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *__restrict__ nbor, uint8_t *occ5,
                                              int32_t *cnt_all, SwapRecord *rec, uint32_t stream, double cur,
-                                             int tasks, int depth, int64_t max_rounds, McTrace tr)
+                                             int tasks, int depth, int64_t max_rounds, McTrace tr,
+                                             McResume rs = McResume{0, 0, 0ull, -1.0})
 {
     constexpr int S = L::S, NC = S * T * T, NCP = mc_ncount_pad(NC);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     int32_t *cnt = cnt_all + warp * NCP;  // this warp's copy of the counts
-    int miss = 0;
-    int64_t round = 0, accepts = 0, evals = 0;
-    while (miss < depth && round < max_rounds) {
+    int miss = rs.miss0;
+    int64_t round = rs.round0, accepts = 0, evals = 0;
+    bool yielded = false;
+    while (miss < depth && round < max_rounds && !(kYield && cur <= rs.tol2)) {
         SwapRecord *rr = rec + (round & 1) * nwarps;
         SwapRecord &mine = rr[warp];  // this warp's best proposal of the round
         if (lane == 0) {
@@ -510,7 +527,10 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
             }
             __syncwarp();
         }
+        // the stop decision travels in warp 0's record (read by all after the barrier)
+        if (kYield && tid == 0) rr[0].pad_ = (rs.deadline_ns && global_ns() >= rs.deadline_ns) ? 1 : 0;
         __syncthreads();
+        const bool stop = kYield && rr[0].pad_ != 0;
         // every warp reduces the records of all warps
         double xf = lane < nwarps ? rr[lane].f2 : inf_d();
         int xq = lane < nwarps ? rr[lane].task : 0x7FFFFFFF;
@@ -564,9 +584,13 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
             ++miss;
         }
         ++round;
+        if (kYield && stop && miss < depth && round < max_rounds && !(cur <= rs.tol2)) {
+            yielded = true;
+            break;
+        }
     }
     __syncthreads();
-    return McTally{cur, round, accepts, evals};
+    return McTally{cur, round - rs.round0, accepts, evals, round, miss, yielded};
 }
 
 // Slot row (species bytes) -> 5*species in shared memory (16-byte vectors).

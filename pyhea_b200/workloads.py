@@ -16,6 +16,9 @@ pair-probability matrix (sum_j c_j alpha_ij = 0).
               P=64, Q=256 (I=10, D=10)
   large       FCC 100^3 (4,000,000 sites, 12/6/24), 4 species at 0.25, alpha ~
               U(-0.05, 0.05) with zero row sums; P=32, Q=4096, I=200, D=20
+  serving     Poisson request stream; FCC/BCC supercells with log-uniform site
+              counts in [4e3, 1e6], 3-6 species (Dirichlet(2)), projected
+              alpha ~ U(-0.1, 0.1)
 """
 import numpy as np
 
@@ -134,6 +137,36 @@ def large(seed=0):
     rng = np.random.default_rng(seed)
     return Structure(_lat.FCC, 100, _lat.SHELLS_FCC_TRUE3, [1_000_000] * 4, WEIGHTS,
                      zero_row_sum_target(rng, 4, 0.05), P=32, Q=4096, I=200, D=20, name="fcc100_t4_12-6-24")
+
+
+def serving(seed=0, rate=200.0, duration=60.0, P=8, Q=256, I=4, D=10, n_min=4e3, n_max=1e6):
+    """Request stream of the serving loop: Poisson arrivals at `rate` per second
+    for `duration` seconds; each request an FCC/BCC (p=0.5) supercell whose site
+    count is log-uniform in [n_min, n_max] (rounded to the nearest cubic cell
+    inside the range), 3-6 species with Dirichlet(2) compositions, alpha ~
+    U(-0.1, 0.1) projected onto sum_j c_j alpha_ij = 0.  Returns a list of
+    (arrival seconds, Structure)."""
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            return out
+        lat = _lat.FCC if rng.random() < 0.5 else _lat.BCC
+        nb = 4 if lat == _lat.FCC else 2
+        n_goal = float(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
+        cell = max(2, int(round((n_goal / nb) ** (1.0 / 3.0))))
+        while nb * cell ** 3 > n_max and cell > 2:
+            cell -= 1
+        while nb * cell ** 3 < n_min:
+            cell += 1
+        n = nb * cell ** 3
+        T = int(rng.integers(3, 7))
+        species = dirichlet_counts(rng, T, n)
+        target = projected_target(rng, species / n, 0.1)
+        shells = _lat.SHELLS_FCC_TRUE3 if lat == _lat.FCC else _lat.SHELLS_REFERENCE
+        out.append((t, Structure(lat, cell, shells, species, WEIGHTS, target, P=P, Q=Q, I=I, D=D,
+                                 name=f"{'fcc' if lat == _lat.FCC else 'bcc'}{cell}_t{T}")))
 
 
 def small_case(lattice=_lat.FCC, cell=4, species=(64, 64, 64, 64), shells=3, shell_set=_lat.SHELLS_REFERENCE, seed=0,
