@@ -70,6 +70,8 @@ struct BatchStruct {
     double *f2;
     int32_t *order;    // [2P] slot ids
     int32_t *scratch;  // [2P] sort scratch
+    uint4 *hist;       // [2P][N] site histograms
+    const uint32_t *nbmask;
     int32_t P, Q, D, I;
     int64_t max_rounds;
     double tol2;  // tolerance on f2 (< 0: none): local searches and the structure end once reached
@@ -250,6 +252,7 @@ __device__ __noinline__ JobEnd batch_job(const SearchConst &c, const BatchStruct
     const int slot = __ldcg(d.order + (job.kind == kJobGenMc ? P + pos : pos));
     uint8_t *gocc = d.occ + (size_t)slot * c.occ_stride;
     int32_t *gcnt = d.cnt + (size_t)slot * NC;
+    uint4 *hist = d.hist + (size_t)slot * c.num_sites;
     uint8_t *occ5 = hbm ? gocc : smem;
     int32_t *cnt_all = reinterpret_cast<int32_t *>(hbm ? smem : smem + c.occ_stride + 16);
     SwapRecord *rec = reinterpret_cast<SwapRecord *>(cnt_all + nwarps * NCP);
@@ -267,7 +270,7 @@ __device__ __noinline__ JobEnd batch_job(const SearchConst &c, const BatchStruct
         generate_occupancy<T>(c, (uint32_t)pos, generation, occ5, (job.kind == kJobGen0 && !hbm) ? gocc : nullptr);
         if (threadIdx.x == 0) occ5[n] = 0;
         __syncthreads();
-        block_recount<T, S>(c, d.nbor, occ5, cnt_all);  // copy 0; ends with a barrier
+        block_recount<T, S>(c, d.nbor, occ5, cnt_all, hist);  // copy 0; ends with a barrier
         cur = fitness_of_counts<T, S>(c, cnt_all);
         if (job.kind == kJobGen0) {
             if (hbm) unstage_occupancy(c, occ5, gocc);
@@ -283,8 +286,9 @@ __device__ __noinline__ JobEnd batch_job(const SearchConst &c, const BatchStruct
     const uint32_t call = job.kind == kJobMc2 ? (uint32_t)(2 * job.iter + 1) : (uint32_t)(2 * job.iter);
     const uint32_t stream = (call << 16) | (uint32_t)pos;
     const McResume rs{job.resume ? (int64_t)job.round0 : 0, job.resume ? job.miss0 : 0, deadline, d.tol2};
-    const McTally t = mc_rounds<T, L, HEA_BATCH_AHEAD, true>(c, d.nbor, occ5, cnt_all, rec, stream, cur, d.Q, d.D,
-                                                             d.max_rounds, McTrace{nullptr, nullptr, 0}, rs);
+    const McTally t = mc_rounds<T, L, HEA_BATCH_AHEAD, true, HEA_SITE_HIST != 0>(
+        c, d.nbor, occ5, cnt_all, rec, stream, cur, d.Q, d.D, d.max_rounds, McTrace{nullptr, nullptr, 0}, rs, hist,
+        d.nbmask);
     unstage_occupancy(c, occ5, gocc);  // in place when hbm
     if (warp == 0)
         for (int x = lane; x < NC; x += 32) gcnt[x] = cnt_all[x];

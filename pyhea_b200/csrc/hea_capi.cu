@@ -183,6 +183,22 @@ __global__ void pad_and_check_kernel(const int32_t *raw, int32_t *padded, PadGeo
     }
 }
 
+// Bit (n - s + N - 1) for every entry n (< N) of every site s of the padded
+// table: the site-id offsets at which two sites can be neighbours.
+__global__ void nbmask_kernel(const int32_t *padded, int num_sites, int pad_row, uint32_t *mask)
+{
+    const int64_t total = (int64_t)num_sites * pad_row;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
+        const int sidx = (int)(x / pad_row);
+        const int n = padded[x];
+        if (n < 0 || n >= num_sites) continue;
+        const uint32_t d = (uint32_t)(n - sidx + num_sites - 1);
+        atomicOr(mask + (d >> 5), 1u << (d & 31u));
+    }
+}
+
+size_t nbmask_words(int num_sites) { return ((size_t)2 * num_sites - 1 + 31) / 32; }
+
 __global__ void gather_rows_kernel(const uint8_t *occ, const int32_t *order, int count, int stride, int n,
                                    const double *f2, uint8_t *out, double *out_f2)
 {
@@ -315,6 +331,7 @@ struct DeviceTables {
     int T = 0, S = 0, N = 0;
     int64_t ncount = 0;
     int4 *nbor = nullptr;
+    uint32_t *nbmask = nullptr;  // neighbour-offset bitmap (nbmask_kernel)
     size_t smem_gen = 0, smem_mc = 0;
     GenFn gen = nullptr;
     McFn mc = nullptr;
@@ -326,6 +343,7 @@ struct DeviceTables {
     ~DeviceTables()
     {
         if (nbor) cudaFree(nbor);
+        if (nbmask) cudaFree(nbmask);
     }
 };
 
@@ -514,6 +532,12 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t
         return fail(HEA_ERR_UNSUPPORTED,
                     "neighbour list is not symmetric within a shell (site a lists b a different number of times "
                     "than b lists a)");
+    const size_t words = nbmask_words(N);
+    if (cudaMalloc(&dt.nbmask, words * sizeof(uint32_t)) != cudaSuccess)
+        return fail(HEA_ERR_NOMEM, "cannot allocate the neighbour-offset bitmap");
+    HEA_CUDA(cudaMemset(dt.nbmask, 0, words * sizeof(uint32_t)));
+    nbmask_kernel<<<1184, 256>>>(reinterpret_cast<const int32_t *>(dt.nbor), N, poff, dt.nbmask);
+    HEA_CUDA(cudaGetLastError());
     return HEA_OK;
 }
 
@@ -540,6 +564,7 @@ struct hea_plan {
     uint8_t *occ = nullptr, *out_occ = nullptr;
     int32_t *cnt = nullptr, *order = nullptr, *scratch = nullptr;
     double *f2 = nullptr, *out_f2 = nullptr;
+    uint4 *hist = nullptr;  // [slots][N] site histograms (not for the HBM cluster path)
     unsigned long long *stats = nullptr;
     std::vector<cudaEvent_t> mc_events;  // start/stop pairs, HEA_FLAG_TIME_KERNELS
     int mc_timed = 0;
@@ -549,7 +574,7 @@ struct hea_plan {
         for (cudaEvent_t e : joins) cudaEventDestroy(e);
         if (side) cudaStreamDestroy(side);
         for (void *p : {(void *)occ, (void *)out_occ, (void *)cnt, (void *)order, (void *)scratch, (void *)f2,
-                        (void *)out_f2, (void *)stats})
+                        (void *)out_f2, (void *)stats, (void *)hist})
             if (p) cudaFree(p);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -571,6 +596,7 @@ int launch_generate(hea_plan *pl, const int32_t *order, int count, uint32_t gene
     a.order = order;
     a.generation = generation;
     a.generate = generate;
+    a.hist = pl->hist;
     if (pl->dt.large) {
         const SearchConst &c = pl->dt.c;
         int chunks = (c.num_sites + 255) / 256;
@@ -597,6 +623,8 @@ int launch_mc(hea_plan *pl, const int32_t *order, int count, uint32_t mc_call, M
     a.cnt = pl->cnt;
     a.f2 = pl->f2;
     a.order = order;
+    a.hist = pl->hist;
+    a.nbmask = pl->dt.nbmask;
     a.mc_call = mc_call;
     a.tasks = pl->prm.parallel_task;
     a.depth = pl->prm.converge_depth;
@@ -665,6 +693,10 @@ int plan_alloc(hea_plan *pl, int slots)
         cudaMalloc(&pl->out_f2, (size_t)slots * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&pl->stats, 4 * sizeof(unsigned long long)) != cudaSuccess)
         return fail(HEA_ERR_NOMEM, "cannot allocate the population buffers (%zu bytes of occupancy)", occ_bytes);
+    if (!pl->dt.large && HEA_SITE_HIST &&
+        cudaMalloc(&pl->hist, (size_t)slots * c.num_sites * sizeof(uint4)) != cudaSuccess)
+        return fail(HEA_ERR_NOMEM, "cannot allocate the site histograms (%zu bytes)",
+                    (size_t)slots * c.num_sites * sizeof(uint4));
     HEA_CUDA(cudaMemsetAsync(pl->occ, 0, occ_bytes, pl->stream));
     iota_kernel<<<(slots + 255) / 256, 256, 0, pl->stream>>>(pl->order, slots);
     HEA_CUDA(cudaGetLastError());
@@ -1344,6 +1376,8 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
         if ((rc = batch_alloc(b, &d.f2, (size_t)slots * sizeof(double))) != HEA_OK) break;
         if ((rc = batch_alloc(b, &d.order, (size_t)slots * sizeof(int32_t))) != HEA_OK) break;
         if ((rc = batch_alloc(b, &d.scratch, (size_t)slots * sizeof(int32_t))) != HEA_OK) break;
+        if ((rc = batch_alloc(b, &d.hist, (size_t)slots * t->N * sizeof(uint4))) != HEA_OK) break;
+        d.nbmask = t->nbmask;
         if (cudaMemset(d.occ, 0, (size_t)slots * t->c.occ_stride) != cudaSuccess) {
             rc = fail(HEA_ERR_CUDA, "cudaMemset failed");
             break;
@@ -1591,7 +1625,7 @@ struct ServerRequest {
 // Arena bytes of a request: padded table, then 2P occupancy rows, counts,
 // f2, order and sort scratch, each 256-byte aligned.
 struct RequestLayout {
-    size_t nbor, occ, cnt, f2, order, scratch, total;
+    size_t nbor, nbmask, hist, occ, cnt, f2, order, scratch, total;
 };
 
 RequestLayout request_layout(const SearchConst &c, int64_t pad_row, int S, int T, int P)
@@ -1605,6 +1639,8 @@ RequestLayout request_layout(const SearchConst &c, int64_t pad_row, int S, int T
         return at;
     };
     L.nbor = take((size_t)c.num_sites * pad_row * sizeof(int32_t));
+    L.nbmask = take(nbmask_words(c.num_sites) * sizeof(uint32_t));
+    L.hist = take(slots * c.num_sites * sizeof(uint4));
     L.occ = take(slots * c.occ_stride);
     L.cnt = take(slots * (size_t)S * T * T * sizeof(int32_t));
     L.f2 = take(slots * sizeof(double));
@@ -1752,6 +1788,12 @@ int server_place(hea_server *sv, ServerRequest &r, int slot)
                                                             sv->d_err + slot);
         e = cudaGetLastError();
     }
+    if (e == cudaSuccess) e = cudaMemsetAsync(base + L.nbmask, 0, L.hist - L.nbmask, sv->stream);
+    if (e == cudaSuccess) {
+        nbmask_kernel<<<1184, 256, 0, sv->stream>>>((const int32_t *)(base + L.nbor), r.N, g.pad_row,
+                                                     (uint32_t *)(base + L.nbmask));
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.occ, 0, L.cnt - L.occ, sv->stream);
     if (e != cudaSuccess) {
         sv->heap.release(off, L.total);
@@ -1765,6 +1807,8 @@ int server_place(hea_server *sv, ServerRequest &r, int slot)
     d.f2 = reinterpret_cast<double *>(base + L.f2);
     d.order = reinterpret_cast<int32_t *>(base + L.order);
     d.scratch = reinterpret_cast<int32_t *>(base + L.scratch);
+    d.hist = reinterpret_cast<uint4 *>(base + L.hist);
+    d.nbmask = reinterpret_cast<const uint32_t *>(base + L.nbmask);
     d.P = P;
     d.Q = r.params.parallel_task;
     d.D = r.params.converge_depth;

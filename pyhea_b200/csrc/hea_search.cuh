@@ -59,6 +59,8 @@ struct McArgs {
     uint8_t *occ;
     int32_t *cnt;
     double *f2;
+    uint4 *hist;              // [slots][N] site histograms (see block_recount)
+    const uint32_t *nbmask;   // neighbour-offset bitmap (see score_swap_hist)
     const int32_t *order;  // slots searched by this launch, one CTA each
     uint32_t mc_call;
     int32_t tasks, depth;
@@ -77,6 +79,7 @@ struct GenArgs {
     uint8_t *occ;
     int32_t *cnt;
     double *f2;
+    uint4 *hist;  // [slots][N] site histograms written by the recount (nullptr: none)
     const int32_t *order;
     uint32_t generation;
     int32_t generate;  // 1: draw a new occupancy; 0: recount the stored one
@@ -262,6 +265,73 @@ __device__ __forceinline__ double score_swap(const SearchConst &c, const int4 *_
     return f2;
 }
 
+// Score one proposal from the site histograms: H(s1) and H(s2) are the
+// neighbourhood histograms h1, h2 of score_swap, so only m (how often s2 is
+// listed among s1's shell-k neighbours) needs the table.  nbmask has bit
+// (n - s + N - 1) set for every table entry n of every site s; a clear bit for
+// s2 - s1 proves m = 0 in every shell, a set bit sends the lane to count s2
+// in s1's row.  Loads go through L2: the accept step updates H with atomics.
+template <int T, class L>
+__device__ __forceinline__ double score_swap_hist(const SearchConst &c, const int4 *__restrict__ nbor,
+                                                  const uint4 *hist, const uint32_t *__restrict__ nbmask,
+                                                  const int32_t *cnt, uint32_t s1, uint32_t s2, int a, int b,
+                                                  uint32_t (&h1)[L::S], uint32_t (&h2)[L::S], int (&m)[L::S])
+{
+    constexpr int S = L::S;
+    const uint4 p = __ldcg(hist + s1), q = __ldcg(hist + s2);
+    const uint32_t d = s2 - s1 + (uint32_t)c.num_sites - 1u;
+    const bool near = (__ldg(nbmask + (d >> 5)) >> (d & 31u)) & 1u;
+    const uint32_t pv[3] = {p.x, p.y, p.z}, qv[3] = {q.x, q.y, q.z};
+#pragma unroll
+    for (int k = 0; k < S; ++k) {
+        h1[k] = pv[k];
+        h2[k] = qv[k];
+        m[k] = 0;
+    }
+    if (near) {
+        const int row4 = L::kRuntime ? c.row4 : L::kRow4;
+        const int4 *r1 = nbor + (size_t)s1 * row4;
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+            const int o = L::kRuntime ? c.off4[k] : L::off(k), n = L::kRuntime ? c.chunks[k] : L::chunks(k);
+            for (int ch = 0; ch < n; ++ch) m[k] += count4(__ldg(r1 + o + ch), s2);
+        }
+    }
+    double f2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < S; ++k) {
+        int u[T];
+        delta_vector<T>(h1[k], h2[k], m[k], a, b, u);
+        f2 = __fma_rn(c.w[k], shell_error<T>(c, cnt, k, u, a, b), f2);
+    }
+    return f2;
+}
+
+// After an accepted swap of s1 (species a -> b) and s2 (b -> a): update the
+// histograms of every neighbour listed in both rows (block-wide, atomics in
+// L2; the caller's barrier publishes them).  An entry n in shell k of s1's row
+// means s1 is in n's shell k as often, since tables are symmetric per shell.
+template <class L>
+__device__ __forceinline__ void update_hist(const SearchConst &c, const int4 *__restrict__ nbor, uint4 *hist,
+                                            uint32_t s1, uint32_t s2, int a, int b)
+{
+    const int row4 = L::kRuntime ? c.row4 : L::kRow4;
+    const int row = 4 * row4;
+    const uint32_t up = (1u << (5 * b)) - (1u << (5 * a));  // s1's neighbours: one a becomes b
+    for (int e = threadIdx.x; e < 2 * row; e += blockDim.x) {
+        const bool first = e < row;
+        const int idx = first ? e : e - row;
+        const int32_t *r = reinterpret_cast<const int32_t *>(nbor + (size_t)(first ? s1 : s2) * row4);
+        const int n = __ldg(r + idx);
+        if (n >= c.num_sites) continue;  // sentinel padding
+        int k = 0;
+#pragma unroll
+        for (int kk = 1; kk < L::S; ++kk) k += idx >= 4 * (L::kRuntime ? c.off4[kk] : L::off(kk));
+        uint32_t *h = reinterpret_cast<uint32_t *>(hist + n) + k;
+        atomicAdd(h, first ? up : 0u - up);
+    }
+}
+
 // Two attempts per Philox call: (x0, x1) then (x2, x3); valid when both draws
 // accept and the species differ (pyhea/cpp/accelerate.cpp:649-655).
 __device__ __forceinline__ bool draw_pair(const SearchConst &c, uint32_t stream, uint32_t round, uint32_t task,
@@ -301,14 +371,29 @@ __device__ __forceinline__ void warp_argmin(double &f, int &q)
     }
 }
 
+// Exact site histogram (5-bit field per species) from the recount's 10-bit
+// fields, less the sentinel entries the padding added to species 0.
+template <int T>
+__device__ __forceinline__ uint32_t pack_hist5(uint64_t h10, int pad)
+{
+    uint32_t r = 0;
+#pragma unroll
+    for (int t = 0; t < T; ++t) r |= (uint32_t)((h10 >> (10 * t)) & 1023u) << (5 * t);
+    return r - (uint32_t)pad;
+}
+
 // ---------------------------------------------------------------------------
 // Block recount of the pair counts of the occupancy in shared memory.
+// With `hist`, also writes every site's histograms: hist[s] = {H_0, H_1, H_2,
+// 0}, H_k = sum over s's shell-k neighbours n of 1 << (5 species(n)) -- the
+// species histogram of the neighbourhood, one 5-bit field per species.
 // Per-thread packed 10-bit accumulators [T][S], flushed to shared-memory bins
 // every 32 sites (32 sites * 28 entries < 1024).  Sentinel entries land in
 // field 0 and are removed at the end (pad_k * n_i per row i).
 // ---------------------------------------------------------------------------
 template <int T, int S>
-__device__ void block_recount(const SearchConst &c, const int4 *__restrict__ nbor, const uint8_t *occ5, int32_t *cnt)
+__device__ void block_recount(const SearchConst &c, const int4 *__restrict__ nbor, const uint8_t *occ5, int32_t *cnt,
+                              uint4 *hist = nullptr)
 {
     for (int x = threadIdx.x; x < S * T * T; x += blockDim.x) cnt[x] = 0;
     __syncthreads();
@@ -334,6 +419,7 @@ __device__ void block_recount(const SearchConst &c, const int4 *__restrict__ nbo
     for (int s = threadIdx.x; s < c.num_sites; s += blockDim.x) {
         const int a5 = occ5[s];
         const int4 *row = nbor + (size_t)s * c.row4;
+        uint32_t hs[3] = {0u, 0u, 0u};
 #pragma unroll
         for (int k = 0; k < S; ++k) {
             uint64_t h = 0;
@@ -346,7 +432,9 @@ __device__ void block_recount(const SearchConst &c, const int4 *__restrict__ nbo
 #pragma unroll
             for (int i = 0; i < T; ++i)
                 if (a5 == 5 * i) acc[i][k] += h;
+            if (hist) hs[k] = pack_hist5<T>(h, c.pad[k]);
         }
+        if (hist) hist[s] = make_uint4(hs[0], hs[1], hs[2], 0u);
         if (++since == 32) {
             flush();
             since = 0;
@@ -406,7 +494,7 @@ __global__ void __launch_bounds__(512, 1) generate_kernel(const SearchConst c, c
     }
     if (threadIdx.x == 0) occ5[n] = 0;
     __syncthreads();
-    block_recount<T, S>(c, g.nbor, occ5, cnt);
+    block_recount<T, S>(c, g.nbor, occ5, cnt, g.hist ? g.hist + (size_t)slot * n : nullptr);
     int32_t *gc = g.cnt + (size_t)slot * S * T * T;
     for (int x = threadIdx.x; x < S * T * T; x += blockDim.x) gc[x] = cnt[x];
     if (threadIdx.x == 0) g.f2[slot] = fitness_of_counts<T, S>(c, cnt);
@@ -469,11 +557,12 @@ struct McResume {
 // is this thread's count.  No barrier at entry; one per round.  occ5 may be
 // shared or global memory; every thread writes the accepted swap's bytes
 // itself, so its own later loads see them either way.
-template <int T, class L, bool kAhead = false, bool kYield = false>
+template <int T, class L, bool kAhead = false, bool kYield = false, bool kHist = false>
 __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *__restrict__ nbor, uint8_t *occ5,
                                              int32_t *cnt_all, SwapRecord *rec, uint32_t stream, double cur,
                                              int tasks, int depth, int64_t max_rounds, McTrace tr,
-                                             McResume rs = McResume{0, 0, 0ull, -1.0})
+                                             McResume rs = McResume{0, 0, 0ull, -1.0}, uint4 *hist = nullptr,
+                                             const uint32_t *nbmask = nullptr)
 {
     constexpr int S = L::S, NC = S * T * T, NCP = mc_ncount_pad(NC);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
@@ -502,7 +591,10 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
                 ++evals;
                 a = occ5[s1] / 5;
                 b = occ5[s2] / 5;
-                f = score_swap<T, L, kAhead>(c, nbor, occ5, cnt, s1, s2, a, b, h1, h2, m);
+                if constexpr (kHist)
+                    f = score_swap_hist<T, L>(c, nbor, hist, nbmask, cnt, s1, s2, a, b, h1, h2, m);
+                else
+                    f = score_swap<T, L, kAhead>(c, nbor, occ5, cnt, s1, s2, a, b, h1, h2, m);
             }
             double wf = f;
             int wq = ok ? q : 0x7FFFFFFF;
@@ -577,6 +669,10 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
                     for (int x = lane; x < NC; x += 32) dst[x] = cnt[x];
                 }
             }
+            if constexpr (kHist) {
+                update_hist<L>(c, nbor, hist, w.s1, w.s2, a, b);
+                __syncthreads();  // next round's proposals read the updated histograms
+            }
             cur = xf;
             miss = 0;
             ++accepts;
@@ -646,6 +742,9 @@ __device__ __forceinline__ void add_tally(const McTally &t, unsigned long long *
     }
 }
 
+#ifndef HEA_SITE_HIST
+#define HEA_SITE_HIST 1  // score proposals from the site histograms (0: gather the neighbours' species)
+#endif
 #ifndef HEA_MC_MIN_BLOCKS
 #define HEA_MC_MIN_BLOCKS 2  // resident 512-thread blocks per SM the register budget aims for
 #endif
@@ -676,8 +775,9 @@ __global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const Search
         tr.counts = g.trace_counts ? g.trace_counts + (size_t)blockIdx.x * g.trace_cap * NC : nullptr;
         tr.cap = g.trace_cap;
     }
-    const McTally t = mc_rounds<T, L>(c, g.nbor, occ5, cnt_all, rec, stream, g.f2[slot], g.tasks, g.depth,
-                                      g.max_rounds, tr);
+    const McTally t = mc_rounds<T, L, false, false, HEA_SITE_HIST != 0>(
+        c, g.nbor, occ5, cnt_all, rec, stream, g.f2[slot], g.tasks, g.depth, g.max_rounds, tr,
+        McResume{0, 0, 0ull, -1.0}, g.hist ? g.hist + (size_t)slot * c.num_sites : nullptr, g.nbmask);
 
     unstage_occupancy(c, occ5, gocc);
     if (warp == 0)
