@@ -104,7 +104,7 @@ McFn pick_mc_large(int T, int c0, int c1, int c2, int S)
 }
 
 using LGenFn = void (*)(const SearchConst, uint8_t *, const int32_t *, uint32_t);
-using LRecFn = void (*)(const SearchConst, const int4 *, const uint8_t *, const int32_t *, int32_t *);
+using LRecFn = void (*)(const SearchConst, const int4 *, const uint8_t *, const int32_t *, int32_t *, uint4 *);
 using LFitFn = void (*)(const SearchConst, const int32_t *, int, const int32_t *, double *);
 const LGenFn kLGen[kMaxTypes + 1] = {nullptr, nullptr, large_generate_kernel<2>, large_generate_kernel<3>,
                                      large_generate_kernel<4>, large_generate_kernel<5>, large_generate_kernel<6>};
@@ -564,7 +564,7 @@ struct hea_plan {
     uint8_t *occ = nullptr, *out_occ = nullptr;
     int32_t *cnt = nullptr, *order = nullptr, *scratch = nullptr;
     double *f2 = nullptr, *out_f2 = nullptr;
-    uint4 *hist = nullptr;  // [slots][N] site histograms (not for the HBM cluster path)
+    uint4 *hist = nullptr;  // [slots][N] site histograms
     unsigned long long *stats = nullptr;
     std::vector<cudaEvent_t> mc_events;  // start/stop pairs, HEA_FLAG_TIME_KERNELS
     int mc_timed = 0;
@@ -604,7 +604,7 @@ int launch_generate(hea_plan *pl, const int32_t *order, int count, uint32_t gene
         if (chunks > cap) chunks = cap;
         zero_counts_kernel<<<dim3(1, count), 128, 0, st>>>(order, count, pl->cnt, (int)pl->dt.ncount);
         if (generate) pl->dt.lgen<<<dim3(chunks, count), 256, 0, st>>>(c, pl->occ, order, generation);
-        pl->dt.lrec<<<dim3(chunks, count), 256, 0, st>>>(c, pl->dt.nbor, pl->occ, order, pl->cnt);
+        pl->dt.lrec<<<dim3(chunks, count), 256, 0, st>>>(c, pl->dt.nbor, pl->occ, order, pl->cnt, pl->hist);
         pl->dt.lfit<<<(count + 127) / 128, 128, 0, st>>>(c, order, count, pl->cnt, pl->f2);
         HEA_CUDA(cudaGetLastError());
         return HEA_OK;
@@ -693,8 +693,7 @@ int plan_alloc(hea_plan *pl, int slots)
         cudaMalloc(&pl->out_f2, (size_t)slots * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&pl->stats, 4 * sizeof(unsigned long long)) != cudaSuccess)
         return fail(HEA_ERR_NOMEM, "cannot allocate the population buffers (%zu bytes of occupancy)", occ_bytes);
-    if (!pl->dt.large && HEA_SITE_HIST &&
-        cudaMalloc(&pl->hist, (size_t)slots * c.num_sites * sizeof(uint4)) != cudaSuccess)
+    if (HEA_SITE_HIST && cudaMalloc(&pl->hist, (size_t)slots * c.num_sites * sizeof(uint4)) != cudaSuccess)
         return fail(HEA_ERR_NOMEM, "cannot allocate the site histograms (%zu bytes)",
                     (size_t)slots * c.num_sites * sizeof(uint4));
     HEA_CUDA(cudaMemsetAsync(pl->occ, 0, occ_bytes, pl->stream));

@@ -13,7 +13,10 @@
 //   * every CTA writes the accepted swap's two bytes itself, so a CTA's L1
 //     never holds a stale copy of its solution's row (the only writes to the
 //     row during the search are those swaps);
-//   * generation and recount are grid-wide over sites (many CTAs per solution).
+//   * generation and recount are grid-wide over sites (many CTAs per solution);
+//     the recount also writes the site histograms the search scores from
+//     (hist, see score_swap_hist), which rank 0 of the cluster updates after
+//     every accepted swap, followed by a cluster barrier.
 #pragma once
 #include <cooperative_groups.h>
 
@@ -47,11 +50,14 @@ __global__ void __launch_bounds__(256) large_generate_kernel(const SearchConst c
 }
 
 // Pair counts of slot rows order[pos] (species bytes), accumulated into
-// cnt[order[pos]] (zeroed by the caller).  grid = (chunks, count); each CTA
-// counts a range of sites into shared bins and adds them once.
+// cnt[order[pos]] (zeroed by the caller), and, with `hist`, the site
+// histograms of those rows (hist + slot * N; see block_recount).  grid =
+// (chunks, count); each CTA counts a range of sites into shared bins and adds
+// them once.
 template <int T, int S>
 __global__ void __launch_bounds__(256) large_recount_kernel(const SearchConst c, const int4 *__restrict__ nbor,
-                                                            const uint8_t *occ, const int32_t *order, int32_t *cnt)
+                                                            const uint8_t *occ, const int32_t *order, int32_t *cnt,
+                                                            uint4 *hist)
 {
     __shared__ int32_t bins[S * T * T];
     const int slot = order[blockIdx.y];
@@ -59,9 +65,11 @@ __global__ void __launch_bounds__(256) large_recount_kernel(const SearchConst c,
     for (int x = threadIdx.x; x < S * T * T; x += blockDim.x) bins[x] = 0;
     __syncthreads();
     const int n = c.num_sites;
+    uint4 *hs = hist ? hist + (size_t)slot * n : nullptr;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         const int a = row[s];
         const int4 *r = nbor + (size_t)s * c.row4;
+        uint32_t hk[3] = {0u, 0u, 0u};
 #pragma unroll
         for (int k = 0; k < S; ++k) {
             uint32_t h = 0;
@@ -75,7 +83,9 @@ __global__ void __launch_bounds__(256) large_recount_kernel(const SearchConst c,
                 const int v = (int)((h >> (5 * t)) & 31u);
                 if (v) atomicAdd(&bins[(k * T + a) * T + t], v);
             }
+            hk[k] = h - (uint32_t)c.pad[k];  // sentinel entries counted as species 0
         }
+        if (hs) hs[s] = make_uint4(hk[0], hk[1], hk[2], 0u);
     }
     __syncthreads();
     int32_t *g = cnt + (size_t)slot * S * T * T;
@@ -119,6 +129,7 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
     const int slot = g.order[sol];
     const uint32_t stream = (g.mc_call << 16) | (uint32_t)sol;
     uint8_t *row = g.occ + (size_t)slot * c.occ_stride;
+    uint4 *hist = g.hist ? g.hist + (size_t)slot * c.num_sites : nullptr;
     int32_t *gcnt = g.cnt + (size_t)slot * NC;
     const int n = c.num_sites;
     // this CTA's share of the row and of the tasks
@@ -152,7 +163,10 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
                 ++evals;
                 a = row[s1] / 5;
                 b = row[s2] / 5;
-                f = score_swap<T, L>(c, g.nbor, row, cnt, s1, s2, a, b, h1, h2, m);
+                if constexpr (HEA_SITE_HIST != 0)
+                    f = score_swap_hist<T, L>(c, g.nbor, hist, g.nbmask, cnt, s1, s2, a, b, h1, h2, m);
+                else
+                    f = score_swap<T, L>(c, g.nbor, row, cnt, s1, s2, a, b, h1, h2, m);
             }
             double wf = f;
             int wq = ok ? q : 0x7FFFFFFF;
@@ -246,6 +260,10 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
                     int32_t *dst = g.trace_counts + ((size_t)sol * g.trace_cap + accepts) * NC;
                     for (int x = lane; x < NC; x += 32) dst[x] = cnt[x];
                 }
+            }
+            if constexpr (HEA_SITE_HIST != 0) {
+                if (rank == 0) update_hist<L>(c, g.nbor, hist, w.s1, w.s2, a, b);
+                cluster.sync();  // the cluster's next proposals read the updated histograms
             }
             cur = xf;
             miss = 0;
