@@ -151,7 +151,8 @@ typedef struct hea_server_config {
     int32_t ring_jobs;     /* job-ring slots per priority level (0: 65536)                        */
     int64_t arena_bytes;   /* device memory for tables and populations (0: 8 GiB or half the free memory) */
     int32_t smem_bytes;    /* shared memory per CTA; larger structures keep occupancy in HBM (0: auto) */
-    int32_t hbm_sites;     /* structures with at least this many sites keep occupancy in HBM too (0: none) */
+    int32_t hbm_sites;     /* occupancy in HBM for structures of at least this many sites; 0: all (the
+                              default, fastest with histogram scoring); -1: only those beyond smem_bytes */
     double slice_ms;       /* length of one step's launch (0: 10 ms)                             */
 } hea_server_config;
 

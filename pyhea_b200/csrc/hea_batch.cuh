@@ -37,11 +37,12 @@
 // by wall time since the last finished job; on expiry the kernel sets an
 // error flag and every CTA returns.
 //
-// Structures whose occupancy does not fit the launch's shared memory keep it
-// in HBM (`hbm`): a job converts the row to 5*species in place (reads through
-// L2, so no stale L1 line of another SM's writes is used; the conversion
-// rewrites every byte this CTA later reads), searches it through L1, and
-// converts it back.
+// Occupancy in HBM (`hbm`, the default: proposals are scored from the site
+// histograms, so a search reads the occupancy only for its draws): a job
+// converts the row to 5*species in place (reads through L2, so no stale L1
+// line of another SM's writes is used; the conversion rewrites every byte this
+// CTA later reads), searches it through L1, and converts it back.  Otherwise
+// the row is staged in the launch's shared memory.
 #pragma once
 #include <cstdint>
 
@@ -315,12 +316,15 @@ __device__ __forceinline__ JobEnd batch_dispatch_t(const SearchConst &c, const B
 #ifndef HEA_BATCH_THREADS
 #define HEA_BATCH_THREADS 256
 #endif
+#ifndef HEA_BATCH_MIN_BLOCKS
+#define HEA_BATCH_MIN_BLOCKS 3  // resident CTAs per SM the register budget aims for (measured: 3 > 2, 4)
+#endif
 
 // The persistent kernel: CTAs take jobs until no structure is active or the
 // launch's deadline has passed.  Dynamic shared memory: occupancy of the
 // largest shared-memory structure + 16 + per-warp counts + swap records; the
 // job's constants (1.9 KB) are copied to static shared memory.
-__global__ void __launch_bounds__(HEA_BATCH_THREADS, 2)
+__global__ void __launch_bounds__(HEA_BATCH_THREADS, HEA_BATCH_MIN_BLOCKS)
     batch_kernel(const BatchStruct *__restrict__ structs, BatchState *states, BatchJob *jobs, BatchCtl *ctl,
                  unsigned long long *finish_ns)
 {

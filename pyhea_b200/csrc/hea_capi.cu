@@ -1313,7 +1313,8 @@ size_t batch_job_smem(int occ_stride, int64_t ncount, int nwarps, bool hbm)
     return (hbm ? 0 : (size_t)occ_stride + 16) + (size_t)nwarps * (4 * mc_ncount_pad((int)ncount) + 2 * sizeof(SwapRecord));
 }
 
-// Dynamic shared memory per CTA that still lets two batch CTAs share an SM.
+// Dynamic shared memory per CTA that still lets HEA_BATCH_MIN_BLOCKS batch CTAs
+// share an SM.
 int batch_smem_budget(size_t *out)
 {
     cudaFuncAttributes a;
@@ -1322,7 +1323,7 @@ int batch_smem_budget(size_t *out)
     HEA_CUDA(cudaGetDevice(&dev));
     HEA_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
     HEA_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
-    long long b = (long long)per_sm / 2 - reserved - (long long)a.sharedSizeBytes;
+    long long b = (long long)per_sm / HEA_BATCH_MIN_BLOCKS - reserved - (long long)a.sharedSizeBytes;
     b &= ~127ll;
     const long long lim = (long long)smem_limit() - (long long)a.sharedSizeBytes;
     *out = (size_t)std::max(0ll, std::min(b, lim));
@@ -1384,13 +1385,16 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
         b->h_structs.push_back(d);
         b->total_jobs += d.I > 0 ? (unsigned long long)P * (2 * d.I + 1) : (unsigned long long)P;
     }
-    // occupancy in shared memory when two CTAs per SM still fit, else in HBM
+    // Occupancy in HBM: with site-histogram scoring a search reads it only for
+    // its draws, and small shared memory leaves room for more CTAs per SM and
+    // a larger L1 (measured faster than staging rows in shared memory).
+    // Without histograms, in shared memory while the per-SM budget allows.
     size_t budget = 0;
     if (rc == HEA_OK) rc = batch_smem_budget(&budget);
     for (int i = 0; rc == HEA_OK && i < count; ++i) {
         BatchStruct &d = b->h_structs[i];
         const int64_t ncount = b->tables[i]->ncount;
-        d.hbm = batch_job_smem(d.c.occ_stride, ncount, nwarps, false) > budget ? 1 : 0;
+        d.hbm = (HEA_SITE_HIST || batch_job_smem(d.c.occ_stride, ncount, nwarps, false) > budget) ? 1 : 0;
         b->smem = std::max(b->smem, batch_job_smem(d.c.occ_stride, ncount, nwarps, d.hbm != 0));
     }
     // priority levels: structures ranked by work, largest first
@@ -1818,7 +1822,7 @@ int server_place(hea_server *sv, ServerRequest &r, int slot)
     d.layout = batch_layout(c, r.S);
     d.level = r.level;
     d.hbm = (batch_job_smem(c.occ_stride, (int64_t)r.S * r.T * r.T, sv->nwarps, false) > sv->smem ||
-             (sv->cfg.hbm_sites > 0 && r.N >= sv->cfg.hbm_sites))
+             sv->cfg.hbm_sites == 0 || (sv->cfg.hbm_sites > 0 && r.N >= sv->cfg.hbm_sites))
                 ? 1
                 : 0;
     r.hbm = d.hbm;
@@ -2008,7 +2012,7 @@ int hea_server_create(const hea_server_config *config, hea_server **out)
     if (rc == HEA_OK) rc = batch_smem_budget(&budget);
     if (rc == HEA_OK) {
         const size_t least = batch_job_smem(0, (int64_t)kMaxShells * kMaxTypes * kMaxTypes, sv->nwarps, true);
-        sv->smem = cfg.smem_bytes > 0 ? (size_t)cfg.smem_bytes : budget;
+        sv->smem = cfg.smem_bytes > 0 ? (size_t)cfg.smem_bytes : (cfg.hbm_sites == 0 ? least : budget);
         sv->smem = std::max(sv->smem, least);
         cudaFuncAttributes a;
         if (cudaFuncGetAttributes(&a, batch_kernel) != cudaSuccess) rc = fail(HEA_ERR_CUDA, "cannot query the batch kernel");

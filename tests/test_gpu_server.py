@@ -50,7 +50,7 @@ def serve_all(srv, ids):
     raise AssertionError("requests did not finish")
 
 
-@pytest.mark.parametrize("slice_ms,hbm_sites", [(50.0, 0), (0.05, 0), (0.2, 1), (0.5, 400)])
+@pytest.mark.parametrize("slice_ms,hbm_sites", [(50.0, -1), (0.05, -1), (0.2, 0), (0.5, 400), (1.0, 1)])
 def test_mix_equals_alone(slice_ms, hbm_sites):
     """Requests arriving over several steps, short slices (searches stop and resume
     many times), and occupancy in HBM for all or some requests."""
@@ -69,7 +69,7 @@ def test_mix_equals_alone(slice_ms, hbm_sites):
         np.testing.assert_array_equal(occ, aocc, err_msg=f"request {rid}")
         np.testing.assert_array_equal(fit, afit, err_msg=f"request {rid}")
         assert info["state"] == 2 and info["iterations"] == q["total_iter"]
-        assert info["hbm"] == (1 if hbm_sites and pb.num_sites >= hbm_sites else 0)
+        assert info["hbm"] == (1 if hbm_sites == 0 or 0 < hbm_sites <= pb.num_sites else 0)
         assert info["finish_ms"] >= info["admit_ms"] >= info["submit_ms"]
     srv.close()
 
