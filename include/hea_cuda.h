@@ -81,6 +81,11 @@ int hea_cuda_available(void);
 /* Message of the calling thread's last failed call ("" if none). */
 const char *hea_last_error(void);
 
+/* Device buffers of finished searches are cached for the next search of the
+ * same shape (up to 8 GiB per process); this returns the current device's
+ * cached buffers to the driver.  No counterpart in the reference. */
+void hea_release_cached_memory(void);
+
 /*
  * The whole search, host buffers in and out: replaces
  * accelerate::gpu::run_local_parallel_hcs_cuda (accelerate.cu:1112-1242).

@@ -96,6 +96,7 @@ def _declare(lib):
     sig = {
         "hea_cuda_available": (_i32, []),
         "hea_last_error": (ctypes.c_char_p, []),
+        "hea_release_cached_memory": (None, []),
         "hea_run_local_parallel_hcs": (_i32, [_P(_Problem), _P(_Params), _P(_u8), _P(_f64), _P(Stats)]),
         "hea_plan_create": (_i32, [_P(_Problem), _P(_Params), _P(ctypes.c_void_p)]),
         "hea_plan_run": (_i32, [ctypes.c_void_p, _u64, _P(Stats)]),

@@ -15,6 +15,7 @@
 #include <map>
 #include <mutex>
 #include <new>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -44,6 +45,106 @@ int fail(int code, const char *fmt, ...)
         cudaError_t e_ = (call);                                                                          \
         if (e_ != cudaSuccess) return fail(HEA_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
+
+// ---------------------------------------------------------------------------
+// Device memory for plans, tables and the component entry points: blocks
+// freed by one call are kept (per device and rounded size) and handed to the
+// next call that asks for the same size, so repeated searches of one shape
+// make no cudaMalloc/cudaFree (both can synchronise the device).  At most
+// kPoolCacheBytes stay cached; a failed cudaMalloc releases the cache and
+// retries.  Blocks go back to the cache only after the owning stream's work
+// has finished (every owner synchronises before freeing).
+// ---------------------------------------------------------------------------
+struct DevicePool {
+    std::mutex mu;
+    std::map<std::pair<int, size_t>, std::vector<void *>> free_;  // (device, rounded size) -> cached blocks
+    std::unordered_map<void *, std::pair<int, size_t>> live;
+    size_t cached = 0;
+};
+// never destroyed: plans may be freed during interpreter or process shutdown
+DevicePool &pool()
+{
+    static DevicePool *p = new DevicePool;
+    return *p;
+}
+constexpr size_t kPoolCacheBytes = (size_t)8 << 30;
+
+size_t pool_round(size_t b)
+{
+    if (b == 0) b = 1;
+    if (b <= ((size_t)1 << 20)) return (b + 4095) & ~(size_t)4095;
+    return (b + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);
+}
+
+void pool_release_device(DevicePool &P, int dev)
+{
+    for (auto it = P.free_.begin(); it != P.free_.end();) {
+        if (it->first.first != dev) {
+            ++it;
+            continue;
+        }
+        for (void *q : it->second) {
+            cudaFree(q);
+            P.cached -= it->first.second;
+        }
+        it = P.free_.erase(it);
+    }
+}
+
+cudaError_t dev_alloc(void **p, size_t bytes)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const size_t r = pool_round(bytes);
+    DevicePool &P = pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    auto it = P.free_.find({dev, r});
+    if (it != P.free_.end() && !it->second.empty()) {
+        *p = it->second.back();
+        it->second.pop_back();
+        P.cached -= r;
+        P.live[*p] = {dev, r};
+        return cudaSuccess;
+    }
+    e = cudaMalloc(p, r);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        pool_release_device(P, dev);
+        e = cudaMalloc(p, r);
+    }
+    if (e == cudaSuccess) P.live[*p] = {dev, r};
+    return e;
+}
+
+template <class X>
+cudaError_t dev_alloc(X **p, size_t bytes)
+{
+    void *q = nullptr;
+    const cudaError_t e = dev_alloc(&q, bytes);
+    *p = static_cast<X *>(q);
+    return e;
+}
+
+void dev_free(void *p)
+{
+    if (!p) return;
+    DevicePool &P = pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    auto it = P.live.find(p);
+    if (it == P.live.end()) {
+        cudaFree(p);
+        return;
+    }
+    const std::pair<int, size_t> key = it->second;
+    P.live.erase(it);
+    if (P.cached + key.second > kPoolCacheBytes) {
+        cudaFree(p);
+        return;
+    }
+    P.free_[key].push_back(p);
+    P.cached += key.second;
+}
 
 #define HEA_TRY(expr)            \
     do {                         \
@@ -342,8 +443,8 @@ struct DeviceTables {
     LFitFn lfit = nullptr;
     ~DeviceTables()
     {
-        if (nbor) cudaFree(nbor);
-        if (nbmask) cudaFree(nbmask);
+        dev_free(nbor);
+        dev_free(nbmask);
     }
 };
 
@@ -510,9 +611,10 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t
     const size_t pad_bytes = (size_t)N * poff * sizeof(int32_t);
     int32_t *raw = nullptr;
     int *derr = nullptr;
-    HEA_CUDA(cudaMalloc(&raw, raw_bytes));
-    if (cudaMalloc(&dt.nbor, pad_bytes) != cudaSuccess || cudaMalloc(&derr, sizeof(int)) != cudaSuccess) {
-        cudaFree(raw);
+    HEA_CUDA(dev_alloc(&raw, raw_bytes));
+    if (dev_alloc(&dt.nbor, pad_bytes) != cudaSuccess || dev_alloc(&derr, sizeof(int)) != cudaSuccess) {
+        dev_free(raw);
+        dev_free(derr);
         return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes for the neighbour table", pad_bytes);
     }
     int herr = 0;
@@ -523,8 +625,8 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaFree(raw);
-    cudaFree(derr);
+    dev_free(raw);
+    dev_free(derr);
     if (e != cudaSuccess) return fail(HEA_ERR_CUDA, "neighbour table upload failed: %s", cudaGetErrorString(e));
     if (herr & 1) return fail(HEA_ERR_INVALID, "neighbour list holds an id outside [0, %d)", N);
     if (herr & 2) return fail(HEA_ERR_UNSUPPORTED, "neighbour list names a site as its own neighbour");
@@ -533,20 +635,18 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t
                     "neighbour list is not symmetric within a shell (site a lists b a different number of times "
                     "than b lists a)");
     const size_t words = nbmask_words(N);
-    if (cudaMalloc(&dt.nbmask, words * sizeof(uint32_t)) != cudaSuccess)
+    if (dev_alloc(&dt.nbmask, words * sizeof(uint32_t)) != cudaSuccess)
         return fail(HEA_ERR_NOMEM, "cannot allocate the neighbour-offset bitmap");
     HEA_CUDA(cudaMemset(dt.nbmask, 0, words * sizeof(uint32_t)));
     nbmask_kernel<<<1184, 256>>>(reinterpret_cast<const int32_t *>(dt.nbor), N, poff, dt.nbmask);
     HEA_CUDA(cudaGetLastError());
+    HEA_CUDA(cudaStreamSynchronize(0));  // callers launch on their own non-blocking streams
     return HEA_OK;
 }
 
 struct DeviceBuf {
     void *p = nullptr;
-    ~DeviceBuf()
-    {
-        if (p) cudaFree(p);
-    }
+    ~DeviceBuf() { dev_free(p); }
 };
 
 }  // namespace
@@ -570,12 +670,14 @@ struct hea_plan {
     int mc_timed = 0;
     ~hea_plan()
     {
+        if (stream) cudaStreamSynchronize(stream);  // buffers return to the pool only when idle
+        if (side) cudaStreamSynchronize(side);
         for (cudaEvent_t e : mc_events) cudaEventDestroy(e);
         for (cudaEvent_t e : joins) cudaEventDestroy(e);
         if (side) cudaStreamDestroy(side);
         for (void *p : {(void *)occ, (void *)out_occ, (void *)cnt, (void *)order, (void *)scratch, (void *)f2,
                         (void *)out_f2, (void *)stats, (void *)hist})
-            if (p) cudaFree(p);
+            dev_free(p);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
@@ -684,16 +786,16 @@ int plan_alloc(hea_plan *pl, int slots)
     HEA_CUDA(cudaEventCreate(&pl->ev0));
     HEA_CUDA(cudaEventCreate(&pl->ev1));
     const size_t occ_bytes = (size_t)slots * c.occ_stride;
-    if (cudaMalloc(&pl->occ, occ_bytes) != cudaSuccess ||
-        cudaMalloc(&pl->cnt, (size_t)slots * pl->dt.ncount * sizeof(int32_t)) != cudaSuccess ||
-        cudaMalloc(&pl->order, (size_t)slots * sizeof(int32_t)) != cudaSuccess ||
-        cudaMalloc(&pl->scratch, (size_t)slots * sizeof(int32_t)) != cudaSuccess ||
-        cudaMalloc(&pl->f2, (size_t)slots * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&pl->out_occ, (size_t)slots * c.num_sites) != cudaSuccess ||
-        cudaMalloc(&pl->out_f2, (size_t)slots * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&pl->stats, 4 * sizeof(unsigned long long)) != cudaSuccess)
+    if (dev_alloc(&pl->occ, occ_bytes) != cudaSuccess ||
+        dev_alloc(&pl->cnt, (size_t)slots * pl->dt.ncount * sizeof(int32_t)) != cudaSuccess ||
+        dev_alloc(&pl->order, (size_t)slots * sizeof(int32_t)) != cudaSuccess ||
+        dev_alloc(&pl->scratch, (size_t)slots * sizeof(int32_t)) != cudaSuccess ||
+        dev_alloc(&pl->f2, (size_t)slots * sizeof(double)) != cudaSuccess ||
+        dev_alloc(&pl->out_occ, (size_t)slots * c.num_sites) != cudaSuccess ||
+        dev_alloc(&pl->out_f2, (size_t)slots * sizeof(double)) != cudaSuccess ||
+        dev_alloc(&pl->stats, 4 * sizeof(unsigned long long)) != cudaSuccess)
         return fail(HEA_ERR_NOMEM, "cannot allocate the population buffers (%zu bytes of occupancy)", occ_bytes);
-    if (HEA_SITE_HIST && cudaMalloc(&pl->hist, (size_t)slots * c.num_sites * sizeof(uint4)) != cudaSuccess)
+    if (HEA_SITE_HIST && dev_alloc(&pl->hist, (size_t)slots * c.num_sites * sizeof(uint4)) != cudaSuccess)
         return fail(HEA_ERR_NOMEM, "cannot allocate the site histograms (%zu bytes)",
                     (size_t)slots * c.num_sites * sizeof(uint4));
     HEA_CUDA(cudaMemsetAsync(pl->occ, 0, occ_bytes, pl->stream));
@@ -856,6 +958,15 @@ hea_params component_params(int count, int tasks, int depth, int64_t max_rounds,
 // ---------------------------------------------------------------------------
 extern "C" {
 
+void hea_release_cached_memory(void)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    DevicePool &P = pool();
+    std::lock_guard<std::mutex> lk(P.mu);
+    pool_release_device(P, dev);
+}
+
 int hea_cuda_available(void)
 {
     int n = 0;
@@ -990,13 +1101,13 @@ int hea_local_search(const hea_problem *problem, uint64_t seed, uint32_t mc_call
     const size_t ncount = (size_t)pl->dt.ncount;
     McArgs extra{};
     if (rc == HEA_OK) {
-        if (cudaMalloc(&drounds.p, count * sizeof(int64_t)) != cudaSuccess) rc = fail(HEA_ERR_NOMEM, "no memory");
+        if (dev_alloc(&drounds.p, count * sizeof(int64_t)) != cudaSuccess) rc = fail(HEA_ERR_NOMEM, "no memory");
         extra.rounds_out = (int64_t *)drounds.p;
         if (rc == HEA_OK && trace_cap > 0) {
-            if (cudaMalloc(&dtrace.p, (size_t)count * trace_cap * sizeof(AcceptRecord)) != cudaSuccess ||
-                cudaMalloc(&dlen.p, count * sizeof(int64_t)) != cudaSuccess ||
+            if (dev_alloc(&dtrace.p, (size_t)count * trace_cap * sizeof(AcceptRecord)) != cudaSuccess ||
+                dev_alloc(&dlen.p, count * sizeof(int64_t)) != cudaSuccess ||
                 (trace_counts &&
-                 cudaMalloc(&dtc.p, (size_t)count * trace_cap * ncount * sizeof(int32_t)) != cudaSuccess))
+                 dev_alloc(&dtc.p, (size_t)count * trace_cap * ncount * sizeof(int32_t)) != cudaSuccess))
                 rc = fail(HEA_ERR_NOMEM, "cannot allocate the trace buffers");
             extra.trace = (AcceptRecord *)dtrace.p;
             extra.trace_counts = (int32_t *)dtc.p;
@@ -1044,7 +1155,7 @@ int hea_build_neighbors(int32_t lattice, int32_t cell, int32_t shell_set, int32_
     if (!out_nbor) return HEA_OK;
     DeviceBuf d, derr;
     const size_t bytes = (size_t)n * row * sizeof(int32_t);
-    if (cudaMalloc(&d.p, bytes) != cudaSuccess || cudaMalloc(&derr.p, sizeof(int)) != cudaSuccess)
+    if (dev_alloc(&d.p, bytes) != cudaSuccess || dev_alloc(&derr.p, sizeof(int)) != cudaSuccess)
         return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes for the neighbour table", bytes);
     HEA_CUDA(cudaMemset(derr.p, 0, sizeof(int)));
     const int blocks = (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
