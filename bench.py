@@ -37,6 +37,10 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes (read + write) per swap evaluation of mc_kernel on the plain GPU workload, from one
+# ncu capture (profiles/mc_kernel_bcc20_t5.md: 160.1 MB over a launch of 203.4 M evaluations);
+# reported per launch as roofline.traffic, scaled by the evaluations of the bench's launches.
+DRAM_BYTES_PER_EVAL = {"plain_gpu": 160.1e6 / 203.4e6}
 
 
 def parse_args():
@@ -491,7 +495,10 @@ def main():
             "e2e": {"value": e2e_evals_all / e2e_max, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "frac": (achieved / peak) if achieved else None,
+                         "traffic": (DRAM_BYTES_PER_EVAL[args.workload] * evals / launches
+                                     if args.workload in DRAM_BYTES_PER_EVAL and launches else None),
+                         "algorithmic_bytes_per_launch": evals * B / launches if launches else None,
                          "kernel": "mc_kernel (local search)", "bytes_per_eval": B, "peak_kind": peak_kind,
                          "kernel_share": mc_ms / total_ms if total_ms else None},
             "search": {"evals_per_step": evals / args.steps, "accepts_per_step": accepts / args.steps,
