@@ -14,6 +14,10 @@ Fixtures written:
   ref_engine.npz     per-case occupancies and swaps with the reference engine's
                      gamma (accelerate.cpp:370-399), full fitness (:118-180) and
                      incremental fitness (:498-570)
+  poscar_*.txt       POSCAR files written by the reference writer
+                     (pyhea/io/output.py:62-106) for seeded occupancies of FCC and
+                     BCC cells (`python tests/golden/make_golden.py poscar` writes
+                     only these)
 
 The reference's Python modules import mpi4py, OVITO, dpdata and matplotlib at
 module level; none is needed by the two functions used here, so they are
@@ -47,8 +51,25 @@ def flat_nbor(nbor):
     return np.array([np.concatenate([np.asarray(sh, dtype=np.int64) for sh in site]) for site in nbor], dtype=np.int32)
 
 
+POSCAR_CASES = [("poscar_fcc3_t4.txt", "FCC", 3, 4, 11), ("poscar_bcc4_t3.txt", "BCC", 4, 3, 12)]
+
+
+def poscar_fixtures(lattice):
+    from pyhea.io.output import write_poscar  # noqa: E402
+
+    for name, typ, L, T, seed in POSCAR_CASES:
+        lat = lattice([L, L, L], typ, 3.6, np.eye(3) * L)
+        n = len(lat.coords)
+        occ = np.random.default_rng(seed).integers(0, T, size=n)
+        write_poscar([int(x) for x in occ], lat, T, [f"E{t}" for t in range(T)], os.path.join(HERE, name))
+
+
 def main():
     lattice, input_config = import_reference()
+    if sys.argv[1:] == ["poscar"]:
+        poscar_fixtures(lattice)
+        return
+    poscar_fixtures(lattice)
 
     # 1. neighbour lists
     nb = {}
