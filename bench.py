@@ -333,6 +333,7 @@ def run_serving(args):
     srv.drain()
     for rid in list(srv._meta):
         srv.result(rid)
+    srv.take_finished()
     base = srv.status()
 
     sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
@@ -357,10 +358,10 @@ def run_serving(args):
             time.sleep(max(0.0, min(reqs[i][0] - now, 0.002)))
             continue
         srv.step()
-        for rid in list(arrival):
-            r = srv.result(rid)
-            if r is None:
+        for rid in srv.take_finished():
+            if rid not in arrival:
                 continue
+            r = srv.result(rid)
             occ, fit, info = r
             t = time.perf_counter() - t0
             lat.append((t - arrival.pop(rid)) * 1000.0)
@@ -432,7 +433,7 @@ def main():
     st = workload(args.workload)
     problem = st.problem(device=True)
     nbor, sizes = st.neighbors(device=True)
-    plan = hb.Plan(problem, st.P, st.I, st.Q, st.D, time_kernels=True)
+    plan = hb.Plan(problem, st.P, st.I, st.Q, st.D, time_kernels=True, autotune=True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     from pyhea_b200 import replicas
 
@@ -457,6 +458,7 @@ def main():
     torch.cuda.synchronize()
     clocks = sampler.stop()
     _, best = plan.read()
+    block = plan.local_search_block
     plan.close()
 
     # end to end through the C ABI with pinned host buffers
@@ -490,7 +492,8 @@ def main():
             "metric": "swap_evals_per_sec", "value": evals_all / (total_ms_max / 1000.0), "unit": "swap-evals/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": dict(config_of(st, args.workload), parallelism=f"replicas x{world}"),
+            "config": dict(config_of(st, args.workload), parallelism=f"replicas x{world}",
+                           local_search_block=block),
             "gpu_launches": None,
             "e2e": {"value": e2e_evals_all / e2e_max, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},

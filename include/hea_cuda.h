@@ -34,6 +34,8 @@ extern "C" {
 #define HEA_FLAG_TIME_KERNELS 2 /* time every local-search launch with CUDA events (hea_stats.mc_ms)        */
 #define HEA_FLAG_HBM_OCCUPANCY 4 /* keep occupancies in HBM and search each solution with a thread-block
                                     cluster -- the path structures too large for shared memory always take */
+#define HEA_FLAG_AUTOTUNE 8     /* plans: time the local search's CTA sizes on short searches at creation
+                                   and keep the fastest (results do not depend on it); cached per shape */
 
 /* One structure to search.  Mirrors the arguments nbor, element, weight and
  * target_sro of run_local_parallel_hcs_cuda (bind.cpp:55-58). */
@@ -108,6 +110,8 @@ int hea_plan_create(const hea_problem *problem, const hea_params *params, hea_pl
 int hea_plan_run(hea_plan *plan, uint64_t seed, hea_stats *stats);
 int hea_plan_read(hea_plan *plan, uint8_t *out_occ, double *out_fitness);
 void hea_plan_destroy(hea_plan *plan);
+/* Threads per CTA of the plan's local search (the autotuner's pick with HEA_FLAG_AUTOTUNE). */
+int32_t hea_plan_local_search_block(const hea_plan *plan);
 
 /*
  * Batched search: `count` independent structures (each with its own problem,
@@ -135,12 +139,14 @@ void hea_batch_destroy(hea_batch *batch);
  * with one, to the same request served alone.  Neither depends on what else
  * was on the GPU or where the time slices fell.
  *
- * submit queues a request on the host (inputs are copied); step admits queued
- * requests in submission order while a request slot, device memory in the
- * arena and job-ring room are free, runs the persistent search kernel for one
- * time slice (slice_ms, or until nothing is active), and collects the requests
- * that finished; result hands over a finished request's population (ascending
- * fitness) and releases it.  tolerance >= 0 (on the reported fitness, sqrt
+ * submit queues a request on the host (inputs are copied); step waits for
+ * the previous time slice, hands over the requests that finished in it,
+ * admits queued requests in submission order while a request slot, device
+ * memory in the arena and job-ring room are free, and launches the persistent
+ * search kernel for the next slice (slice_ms, or until nothing is active)
+ * without waiting for it -- the host's work between steps overlaps the GPU's;
+ * result hands over a finished request's population (ascending fitness) and
+ * releases it.  tolerance >= 0 (on the reported fitness, sqrt
  * of f2): a local search ends once its fitness is <= tolerance, and the
  * request ends once the best fitness after an iteration's survivors' sort
  * is; < 0 runs total_iter iterations.  priority 0..15, 0 first.
@@ -191,6 +197,8 @@ int hea_server_submit_lattice(hea_server *server, int32_t lattice, int32_t cell,
                               const double *target_sro, const hea_params *params, double tolerance,
                               int32_t priority, int64_t *out_id);
 int hea_server_step(hea_server *server, int32_t *out_finished);
+/* Ids of requests that finished (or failed) since the last call, up to cap. */
+int hea_server_take_finished(hea_server *server, int64_t *ids, int32_t cap, int32_t *count);
 int hea_server_result(hea_server *server, int64_t id, uint8_t *out_occ, double *out_fitness,
                       hea_request_info *info);
 int hea_server_info(hea_server *server, int64_t id, hea_request_info *info);

@@ -30,6 +30,7 @@ HEA_OK, HEA_ERR_INVALID, HEA_ERR_UNSUPPORTED, HEA_ERR_CUDA, HEA_ERR_NOMEM, HEA_P
 HEA_FLAG_LOG_ITERS = 1
 HEA_FLAG_TIME_KERNELS = 2
 HEA_FLAG_HBM_OCCUPANCY = 4
+HEA_FLAG_AUTOTUNE = 8
 FCC, BCC = 0, 1
 SHELLS_REFERENCE, SHELLS_FCC_TRUE3 = 0, 1
 
@@ -102,6 +103,7 @@ def _declare(lib):
         "hea_plan_run": (_i32, [ctypes.c_void_p, _u64, _P(Stats)]),
         "hea_plan_read": (_i32, [ctypes.c_void_p, _P(_u8), _P(_f64)]),
         "hea_plan_destroy": (None, [ctypes.c_void_p]),
+        "hea_plan_local_search_block": (_i32, [ctypes.c_void_p]),
         "hea_generate": (_i32, [_P(_Problem), _u64, _u32, _i32, _P(_u8), _P(_i32), _P(_f64)]),
         "hea_recount": (_i32, [_P(_Problem), _i32, _P(_u8), _P(_i32), _P(_f64)]),
         "hea_local_search": (_i32, [_P(_Problem), _u64, _u32, _i32, _i32, _i32, _i64, _P(_u8), _P(_i32), _P(_f64),
@@ -118,6 +120,7 @@ def _declare(lib):
         "hea_server_submit_lattice": (_i32, [ctypes.c_void_p, _i32, _i32, _i32, _i32, _i32, _P(_i32), _P(_f64),
                                              _P(_f64), _P(_Params), _f64, _i32, _P(_i64)]),
         "hea_server_step": (_i32, [ctypes.c_void_p, _P(_i32)]),
+        "hea_server_take_finished": (_i32, [ctypes.c_void_p, _P(_i64), _i32, _P(_i32)]),
         "hea_server_result": (_i32, [ctypes.c_void_p, _i64, _P(_u8), _P(_f64), _P(RequestInfo)]),
         "hea_server_info": (_i32, [ctypes.c_void_p, _i64, _P(RequestInfo)]),
         "hea_server_status_get": (_i32, [ctypes.c_void_p, _P(ServerStatus)]),
@@ -197,13 +200,19 @@ class Plan:
     """Device-resident search (hea_plan_*): tables uploaded once, run many times."""
 
     def __init__(self, problem, num_solutions, total_iter, parallel_task, converge_depth, seed=0, max_rounds=0,
-                 time_kernels=False, hbm_occupancy=False):
+                 time_kernels=False, hbm_occupancy=False, autotune=False):
         self.problem = problem
         self.P = int(num_solutions)
         self._h = ctypes.c_void_p()
-        flags = (HEA_FLAG_TIME_KERNELS if time_kernels else 0) | (HEA_FLAG_HBM_OCCUPANCY if hbm_occupancy else 0)
+        flags = ((HEA_FLAG_TIME_KERNELS if time_kernels else 0) | (HEA_FLAG_HBM_OCCUPANCY if hbm_occupancy else 0)
+                 | (HEA_FLAG_AUTOTUNE if autotune else 0))
         prm = _params(num_solutions, total_iter, parallel_task, converge_depth, seed, max_rounds, flags)
         _check(lib.hea_plan_create(ctypes.byref(problem._c), ctypes.byref(prm), ctypes.byref(self._h)))
+
+    @property
+    def local_search_block(self):
+        """Threads per CTA of the local search (the autotuner's pick when autotune=True)."""
+        return int(lib.hea_plan_local_search_block(self._h))
 
     def run(self, seed):
         st = Stats()
@@ -324,10 +333,18 @@ class Server:
         return rid.value
 
     def step(self):
-        """One admission + time slice + collection; returns the number of requests that finished."""
+        """Wait for the previous time slice, hand over its finished requests, admit queued ones and
+        launch the next slice (not waited for); returns the number of requests that finished."""
         fin = _i32()
         _check(lib.hea_server_step(self._h, ctypes.byref(fin)))
         return fin.value
+
+    def take_finished(self, cap=4096):
+        """Ids of requests that finished (or failed) since the last call."""
+        ids = (_i64 * cap)()
+        n = _i32()
+        _check(lib.hea_server_take_finished(self._h, ids, int(cap), ctypes.byref(n)))
+        return list(ids[: n.value])
 
     def info(self, rid):
         inf = RequestInfo()

@@ -17,6 +17,7 @@
 #include <new>
 #include <unordered_map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "hea_cuda.h"
@@ -668,6 +669,7 @@ struct hea_plan {
     unsigned long long *stats = nullptr;
     std::vector<cudaEvent_t> mc_events;  // start/stop pairs, HEA_FLAG_TIME_KERNELS
     int mc_timed = 0;
+    int mc_block = 0;  // threads per CTA of the local search (choose_block, or the autotuner's pick)
     ~hea_plan()
     {
         if (stream) cudaStreamSynchronize(stream);  // buffers return to the pool only when idle
@@ -755,7 +757,7 @@ int launch_mc(hea_plan *pl, const int32_t *order, int count, uint32_t mc_call, M
         cfg.numAttrs = 1;
         HEA_CUDA(cudaLaunchKernelEx(&cfg, pl->dt.mc, pl->dt.c, a));
     } else {
-        const int block = choose_block(a.tasks);
+        const int block = pl->mc_block;
         pl->dt.mc<<<count, block, mc_smem(pl->dt.c.occ_stride, (int)pl->dt.ncount, block / 32), st>>>(pl->dt.c, a);
     }
     HEA_CUDA(cudaGetLastError());
@@ -920,6 +922,87 @@ int plan_search(hea_plan *pl, hea_stats *stats)
     return HEA_OK;
 }
 
+// Autotuner of the local search's CTA size.  Every CTA size gives the same
+// result (the round's winner is the lexicographic (f2, task) minimum however
+// the tasks are split over warps and passes), so the choice is a pure speed
+// question: each candidate (the default one task per thread, and 256 and 128
+// threads when smaller) searches a fresh generation-0 population for
+// kTuneRounds rounds; the highest evaluations per millisecond wins.  Picks
+// are cached per device and shape for the life of the process.
+struct TuneKey {
+    int dev, N, T, S, row4, Q, P;
+    bool operator<(const TuneKey &o) const
+    {
+        return std::tie(dev, N, T, S, row4, Q, P) < std::tie(o.dev, o.N, o.T, o.S, o.row4, o.Q, o.P);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tune;
+constexpr int kTuneRounds = 48;
+
+// With measure = false only a cached pick is applied (plans created without
+// HEA_FLAG_AUTOTUNE still use the pick of an earlier tuned plan of their shape).
+int plan_autotune(hea_plan *pl, bool measure)
+{
+    if (pl->dt.large) return HEA_OK;  // cluster size follows the task count
+    const SearchConst &c = pl->dt.c;
+    int dev = 0;
+    HEA_CUDA(cudaGetDevice(&dev));
+    const TuneKey key{dev, c.num_sites, pl->dt.T, pl->dt.S, c.row4, pl->prm.parallel_task, pl->P};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            pl->mc_block = it->second;
+            return HEA_OK;
+        }
+    }
+    if (!measure) return HEA_OK;
+    std::vector<int> cand = {choose_block(pl->prm.parallel_task)};
+    for (int b : {256, 128})
+        if (b < cand[0]) cand.push_back(b);
+    int best = cand[0];
+    if (cand.size() > 1) {
+        const hea_params saved = pl->prm;
+        const int64_t cap = saved.max_rounds > 0 ? std::min<int64_t>(saved.max_rounds, kTuneRounds) : kTuneRounds;
+        pl->prm.max_rounds = cap;
+        pl->prm.flags &= ~HEA_FLAG_TIME_KERNELS;
+        double best_rate = -1.0;
+        int rc = HEA_OK;
+        for (int pass = 0; pass < 2 && rc == HEA_OK; ++pass) {  // pass 0 warms up
+            for (int b : cand) {
+                pl->mc_block = b;
+                cudaMemsetAsync(pl->stats, 0, 4 * sizeof(unsigned long long), pl->stream);
+                iota_kernel<<<(2 * pl->P + 255) / 256, 256, 0, pl->stream>>>(pl->order, 2 * pl->P);
+                if ((rc = launch_generate(pl, pl->order, pl->P, 0, 1)) != HEA_OK) break;
+                cudaEventRecord(pl->ev0, pl->stream);
+                if ((rc = launch_mc(pl, pl->order, pl->P, 0, McArgs{})) != HEA_OK) break;
+                cudaEventRecord(pl->ev1, pl->stream);
+                unsigned long long st[4];
+                cudaError_t e = cudaMemcpyAsync(st, pl->stats, sizeof(st), cudaMemcpyDeviceToHost, pl->stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(pl->stream);
+                float ms = 0;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, pl->ev0, pl->ev1);
+                if (e != cudaSuccess) {
+                    rc = fail(HEA_ERR_CUDA, "autotuning failed: %s", cudaGetErrorString(e));
+                    break;
+                }
+                const double rate = ms > 0 ? st[1] / (double)ms : 0.0;
+                if (pass == 1 && rate > best_rate) {
+                    best_rate = rate;
+                    best = b;
+                }
+            }
+        }
+        pl->prm = saved;
+        if (rc != HEA_OK) return rc;
+    }
+    pl->mc_block = best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = best;
+    return HEA_OK;
+}
+
 int plan_create(const hea_problem *pb, const hea_params *prm, int slots, hea_plan **out)
 {
     *out = nullptr;
@@ -929,8 +1012,10 @@ int plan_create(const hea_problem *pb, const hea_params *prm, int slots, hea_pla
     if (rc == HEA_OK) {
         pl->prm = *prm;
         pl->P = prm->num_solutions;
+        pl->mc_block = choose_block(prm->parallel_task);
         rc = plan_alloc(pl, slots);
     }
+    if (rc == HEA_OK) rc = plan_autotune(pl, (prm->flags & HEA_FLAG_AUTOTUNE) != 0);
     if (rc != HEA_OK) {
         delete pl;
         return rc;
@@ -1002,6 +1087,8 @@ int hea_plan_read(hea_plan *plan, uint8_t *out_occ, double *out_fitness)
 }
 
 void hea_plan_destroy(hea_plan *plan) { delete plan; }
+
+int32_t hea_plan_local_search_block(const hea_plan *plan) { return plan ? plan->mc_block : 0; }
 
 int hea_run_local_parallel_hcs(const hea_problem *problem, const hea_params *params, uint8_t *out_occ,
                                double *out_fitness, hea_stats *stats)
@@ -1794,10 +1881,16 @@ struct hea_server {
     size_t raw_bytes = 0;
     void *d_out = nullptr;
     size_t out_bytes = 0;
-    double *d_out_f2 = nullptr;
     std::vector<BatchStruct> h_structs;
-    std::vector<BatchState> h_states;
-    std::vector<unsigned long long> h_finish;
+    BatchState *h_states = nullptr;          // pinned: slice results, copied while the host works
+    unsigned long long *h_finish = nullptr;  // pinned
+    BatchCtl *h_ctl = nullptr;               // pinned
+    uint8_t *h_stage = nullptr;              // pinned staging of finished populations
+    size_t stage_bytes = 0;
+    cudaStream_t side = nullptr;             // copies of finished populations
+    cudaEvent_t ev_gather = nullptr;
+    bool inflight = false;                   // a slice was launched and not yet waited for
+    std::vector<int64_t> finished_ids;       // finished, not yet taken by hea_server_take_finished
     std::vector<int> h_err;
     std::vector<int32_t> h_list;
     std::vector<int64_t> slot_req;                // request id per slot, 0 = free
@@ -1816,11 +1909,16 @@ struct hea_server {
     ~hea_server()
     {
         if (stream) cudaStreamSynchronize(stream);
+        if (side) cudaStreamSynchronize(side);
         for (void *p : buffers) cudaFree(p);
         if (d_raw) cudaFree(d_raw);
         if (d_out) cudaFree(d_out);
+        for (void *p : {(void *)h_states, (void *)h_finish, (void *)h_ctl, (void *)h_stage})
+            if (p) cudaFreeHost(p);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (ev_gather) cudaEventDestroy(ev_gather);
+        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
     }
     double now_ms() const
@@ -1841,6 +1939,7 @@ struct hea_server {
     {
         if (need <= *have) return HEA_OK;
         HEA_CUDA(cudaStreamSynchronize(stream));
+        HEA_CUDA(cudaStreamSynchronize(side));
         if (*p) cudaFree(*p);
         *p = nullptr;
         *have = 0;
@@ -1990,6 +2089,7 @@ int server_admit(hea_server *sv)
                                   : "neighbour list is not symmetric within a shell";
             r.t_finish = t;
             server_release(sv, r);
+            sv->finished_ids.push_back(id);
             continue;
         }
         r.state = 1;
@@ -2008,35 +2108,76 @@ int server_admit(hea_server *sv)
     return HEA_OK;
 }
 
-// Results of the requests that finished in the last slice.
-int server_collect(hea_server *sv, int32_t *finished)
+// Requests that finished in the last slice leave the device: their
+// populations are gathered on the server stream (the GPU is idle between
+// slices), the device copy to pinned staging runs on the side stream while the
+// next slice computes, and their slots and arena memory are released at once
+// (later work on the server stream is ordered after the gathers).
+struct Collect {
+    int64_t id;
+    size_t off, off_f2;
+    int P, N;
+};
+
+int server_collect_start(hea_server *sv, std::vector<Collect> &col)
 {
     const double t = sv->now_ms();
+    size_t total = 0;
     for (int slot = 0; slot < sv->cfg.max_requests; ++slot) {
         const int64_t id = sv->slot_req[slot];
         if (!id || !sv->h_states[slot].done) continue;
         ServerRequest &r = sv->reqs[id];
         if (r.state != 1) continue;
         const BatchStruct &d = sv->h_structs[slot];
-        const size_t rows = (size_t)d.P * d.c.num_sites;
-        HEA_TRY(sv->grow(&sv->d_out, &sv->out_bytes, rows));
-        dim3 grid((unsigned)std::min(64, (d.c.num_sites + 255) / 256), (unsigned)d.P);
-        gather_rows_kernel<<<grid, 256, 0, sv->stream>>>(d.occ, d.order, d.P, d.c.occ_stride, d.c.num_sites, d.f2,
-                                                        (uint8_t *)sv->d_out, sv->d_out_f2);
-        HEA_CUDA(cudaGetLastError());
-        r.occ.resize(rows);
-        r.fit.resize(d.P);
-        HEA_CUDA(cudaMemcpyAsync(r.occ.data(), sv->d_out, rows, cudaMemcpyDeviceToHost, sv->stream));
-        HEA_CUDA(cudaMemcpyAsync(r.fit.data(), sv->d_out_f2, d.P * sizeof(double), cudaMemcpyDeviceToHost, sv->stream));
-        HEA_CUDA(cudaStreamSynchronize(sv->stream));
-        for (double &f : r.fit) f = std::sqrt(f);
-        r.state = 2;
+        Collect c{id, total, 0, d.P, d.c.num_sites};
+        total += ((size_t)d.P * d.c.num_sites + 7) & ~(size_t)7;
+        c.off_f2 = total;
+        total += (size_t)d.P * sizeof(double);
+        col.push_back(c);
         r.t_finish = t;
         r.device_ms = sv->h_finish[slot] * 1e-6;
         r.iterations = sv->h_states[slot].phase;
         for (int k = 0; k < 3; ++k) r.tally[k] = sv->h_states[slot].tally[k];
+    }
+    if (col.empty()) return HEA_OK;
+    HEA_TRY(sv->grow(&sv->d_out, &sv->out_bytes, total));
+    if (total > sv->stage_bytes) {
+        if (sv->h_stage) cudaFreeHost(sv->h_stage);
+        sv->h_stage = nullptr;
+        sv->stage_bytes = 0;
+        if (cudaMallocHost((void **)&sv->h_stage, total) != cudaSuccess)
+            return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes of pinned staging", total);
+        sv->stage_bytes = total;
+    }
+    uint8_t *out = (uint8_t *)sv->d_out;
+    for (const Collect &c : col) {
+        ServerRequest &r = sv->reqs[c.id];
+        const BatchStruct &d = sv->h_structs[r.slot];
+        dim3 grid((unsigned)std::min(64, (c.N + 255) / 256), (unsigned)c.P);
+        gather_rows_kernel<<<grid, 256, 0, sv->stream>>>(d.occ, d.order, c.P, d.c.occ_stride, c.N, d.f2, out + c.off,
+                                                        reinterpret_cast<double *>(out + c.off_f2));
+        HEA_CUDA(cudaGetLastError());
         server_release(sv, r);
         --sv->running;
+    }
+    HEA_CUDA(cudaEventRecord(sv->ev_gather, sv->stream));
+    HEA_CUDA(cudaStreamWaitEvent(sv->side, sv->ev_gather, 0));
+    HEA_CUDA(cudaMemcpyAsync(sv->h_stage, sv->d_out, total, cudaMemcpyDeviceToHost, sv->side));
+    return HEA_OK;
+}
+
+int server_collect_finish(hea_server *sv, const std::vector<Collect> &col, int32_t *finished)
+{
+    if (col.empty()) return HEA_OK;
+    HEA_CUDA(cudaStreamSynchronize(sv->side));
+    for (const Collect &c : col) {
+        ServerRequest &r = sv->reqs[c.id];
+        r.occ.assign(sv->h_stage + c.off, sv->h_stage + c.off + (size_t)c.P * c.N);
+        r.fit.resize(c.P);
+        std::memcpy(r.fit.data(), sv->h_stage + c.off_f2, c.P * sizeof(double));
+        for (double &f : r.fit) f = std::sqrt(f);
+        r.state = 2;
+        sv->finished_ids.push_back(c.id);
         ++sv->finished_total;
         ++*finished;
     }
@@ -2141,12 +2282,9 @@ int hea_server_create(const hea_server_config *config, hea_server **out)
     if (rc == HEA_OK) rc = sv->alloc(&sv->d_finish, sizeof(unsigned long long) * M);
     if (rc == HEA_OK) rc = sv->alloc(&sv->d_list, sizeof(int32_t) * M);
     if (rc == HEA_OK) rc = sv->alloc(&sv->d_err, sizeof(int) * M);
-    if (rc == HEA_OK) rc = sv->alloc(&sv->d_out_f2, sizeof(double) * 65536);
     if (rc == HEA_OK) {
         sv->heap.init((size_t)cfg.arena_bytes);
         sv->h_structs.assign(M, BatchStruct{});
-        sv->h_states.assign(M, BatchState{});
-        sv->h_finish.assign(M, 0);
         sv->h_err.assign(M, 0);
         sv->slot_req.assign(M, 0);
         sv->h_list.reserve(M);
@@ -2156,7 +2294,17 @@ int hea_server_create(const hea_server_config *config, hea_server **out)
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, HEA_BATCH_THREADS, sv->smem);
         if (e == cudaSuccess) e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaMallocHost((void **)&sv->h_states, sizeof(BatchState) * M);
+        if (e == cudaSuccess) e = cudaMallocHost((void **)&sv->h_finish, sizeof(unsigned long long) * M);
+        if (e == cudaSuccess) e = cudaMallocHost((void **)&sv->h_ctl, sizeof(BatchCtl));
+        if (e == cudaSuccess) {
+            std::memset(sv->h_states, 0, sizeof(BatchState) * M);
+            std::memset(sv->h_finish, 0, sizeof(unsigned long long) * M);
+            std::memset(sv->h_ctl, 0, sizeof(BatchCtl));
+        }
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sv->side, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sv->ev_gather, cudaEventDisableTiming);
         if (e == cudaSuccess) e = cudaEventCreate(&sv->ev0);
         if (e == cudaSuccess) e = cudaEventCreate(&sv->ev1);
         if (e == cudaSuccess) e = cudaMemsetAsync(sv->d_states, 0, sizeof(BatchState) * M, sv->stream);
@@ -2240,33 +2388,55 @@ int hea_server_step(hea_server *server, int32_t *out_finished)
     if (out_finished) *out_finished = 0;
     hea_server *sv = server;
     if (!sv->broken.empty()) return server_broken(sv);
-    HEA_TRY(server_admit(sv));
-    if (sv->running == 0) return HEA_OK;
     const int M = sv->cfg.max_requests;
-    HEA_CUDA(cudaEventRecord(sv->ev0, sv->stream));
-    server_arm_kernel<<<1, 1, 0, sv->stream>>>(sv->d_ctl, (unsigned long long)(sv->cfg.slice_ms * 1e6));
-    batch_kernel<<<sv->grid, HEA_BATCH_THREADS, sv->smem, sv->stream>>>(sv->d_structs, sv->d_states, sv->d_jobs,
-                                                                         sv->d_ctl, sv->d_finish);
-    HEA_CUDA(cudaGetLastError());
-    HEA_CUDA(cudaEventRecord(sv->ev1, sv->stream));
-    HEA_CUDA(cudaMemcpyAsync(&sv->last_ctl, sv->d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, sv->stream));
-    HEA_CUDA(cudaMemcpyAsync(sv->h_states.data(), sv->d_states, sizeof(BatchState) * M, cudaMemcpyDeviceToHost,
-                             sv->stream));
-    HEA_CUDA(cudaMemcpyAsync(sv->h_finish.data(), sv->d_finish, sizeof(unsigned long long) * M,
-                             cudaMemcpyDeviceToHost, sv->stream));
-    HEA_CUDA(cudaStreamSynchronize(sv->stream));
-    float ms = 0;
-    HEA_CUDA(cudaEventElapsedTime(&ms, sv->ev0, sv->ev1));
-    sv->busy_ms += ms;
-    ++sv->launches;
-    if (sv->last_ctl.error) {
-        sv->broken = sv->last_ctl.error == 2 ? "a job-ring slot was reused before it was read"
-                                             : "a wait for queued work exceeded its time limit";
-        return server_broken(sv);
+    // 1. the previous slice: wait for it and its state copies
+    if (sv->inflight) {
+        HEA_CUDA(cudaStreamSynchronize(sv->stream));
+        sv->inflight = false;
+        float ms = 0;
+        HEA_CUDA(cudaEventElapsedTime(&ms, sv->ev0, sv->ev1));
+        sv->busy_ms += ms;
+        ++sv->launches;
+        sv->last_ctl = *sv->h_ctl;
+        if (sv->last_ctl.error) {
+            sv->broken = sv->last_ctl.error == 2 ? "a job-ring slot was reused before it was read"
+                                                 : "a wait for queued work exceeded its time limit";
+            return server_broken(sv);
+        }
     }
+    // 2. finished requests: gather, release, copy out behind the next slice
+    std::vector<Collect> col;
+    HEA_TRY(server_collect_start(sv, col));
+    // 3. admission, then the next slice
+    HEA_TRY(server_admit(sv));
+    if (sv->running > 0) {
+        HEA_CUDA(cudaEventRecord(sv->ev0, sv->stream));
+        server_arm_kernel<<<1, 1, 0, sv->stream>>>(sv->d_ctl, (unsigned long long)(sv->cfg.slice_ms * 1e6));
+        batch_kernel<<<sv->grid, HEA_BATCH_THREADS, sv->smem, sv->stream>>>(sv->d_structs, sv->d_states,
+                                                                             sv->d_jobs, sv->d_ctl, sv->d_finish);
+        HEA_CUDA(cudaGetLastError());
+        HEA_CUDA(cudaEventRecord(sv->ev1, sv->stream));
+        HEA_CUDA(cudaMemcpyAsync(sv->h_ctl, sv->d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, sv->stream));
+        HEA_CUDA(cudaMemcpyAsync(sv->h_states, sv->d_states, sizeof(BatchState) * M, cudaMemcpyDeviceToHost,
+                                 sv->stream));
+        HEA_CUDA(cudaMemcpyAsync(sv->h_finish, sv->d_finish, sizeof(unsigned long long) * M,
+                                 cudaMemcpyDeviceToHost, sv->stream));
+        sv->inflight = true;
+    }
+    // 4. hand the finished populations over while the slice runs
     int32_t fin = 0;
-    HEA_TRY(server_collect(sv, &fin));
+    HEA_TRY(server_collect_finish(sv, col, &fin));
     if (out_finished) *out_finished = fin;
+    return HEA_OK;
+}
+
+int hea_server_take_finished(hea_server *server, int64_t *ids, int32_t cap, int32_t *count)
+{
+    if (!server || !count || (cap > 0 && !ids)) return fail(HEA_ERR_INVALID, "server, ids and count are required");
+    const int32_t n = (int32_t)std::min<size_t>(server->finished_ids.size(), cap > 0 ? (size_t)cap : 0);
+    for (int32_t i = 0; i < n; ++i) ids[i] = server->finished_ids[i];
+    server->finished_ids.erase(server->finished_ids.begin(), server->finished_ids.begin() + n);
+    *count = n;
     return HEA_OK;
 }
 

@@ -225,3 +225,20 @@ def test_plans_of_different_sizes_coexist():
     np.testing.assert_array_equal(np.sqrt(hb.recount(pb_big, occ)[1]), fit)
     plan_big.close()
     plan_small.close()
+
+
+def test_autotuned_plan_gives_the_same_search():
+    """The autotuner only picks the local search's CTA size; the search is the same."""
+    st = W.small_case(lattice=L.BCC, cell=6, species=(150, 150, 132), shells=3, seed=3, P=6, Q=384, I=2, D=5)
+    pb = st.problem()
+    ref = hb.Plan(pb, st.P, st.I, st.Q, st.D)
+    tuned = hb.Plan(pb, st.P, st.I, st.Q, st.D, autotune=True)
+    assert ref.local_search_block == 384
+    assert tuned.local_search_block in (384, 256, 128)
+    for seed in (5, 6):
+        a, b = ref.run(seed), tuned.run(seed)
+        assert a["evals"] == b["evals"] and a["accepts"] == b["accepts"]
+        np.testing.assert_array_equal(ref.read()[0], tuned.read()[0])
+        np.testing.assert_array_equal(ref.read()[1], tuned.read()[1])
+    ref.close()
+    tuned.close()
