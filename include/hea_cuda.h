@@ -164,7 +164,7 @@ typedef struct hea_server_config {
     int32_t smem_bytes;    /* shared memory per CTA; larger structures keep occupancy in HBM (0: auto) */
     int32_t hbm_sites;     /* occupancy in HBM for structures of at least this many sites; 0: all (the
                               default, fastest with histogram scoring); -1: only those beyond smem_bytes */
-    double slice_ms;       /* length of one step's launch (0: 10 ms)                             */
+    double slice_ms;       /* length of one step's launch (0: 20 ms)                             */
 } hea_server_config;
 
 typedef struct hea_request_info {

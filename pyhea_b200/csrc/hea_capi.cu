@@ -2248,7 +2248,7 @@ int hea_server_create(const hea_server_config *config, hea_server **out)
     if (config) cfg = *config;
     if (cfg.max_requests <= 0) cfg.max_requests = 256;
     if (cfg.ring_jobs <= 0) cfg.ring_jobs = 65536;
-    if (cfg.slice_ms <= 0) cfg.slice_ms = 10.0;
+    if (cfg.slice_ms <= 0) cfg.slice_ms = 20.0;
     if (cfg.max_requests > 65536) return fail(HEA_ERR_INVALID, "max_requests must be <= 65536");
     if (cfg.ring_jobs > (1 << 26)) return fail(HEA_ERR_INVALID, "ring_jobs must be <= 2^26");
     hea_server *sv = new (std::nothrow) hea_server();
