@@ -249,7 +249,9 @@ def run_batched(args):
                        "l2": "flushed between timed steps (256 MiB write)"},
             "plain": {"value": plain, "ms_per_step": p_ms / args.steps, "evals_per_step": p_ev / args.steps},
             "speedup_vs_plain": value / plain, "identical_structures": same, "structures": len(structs),
-            "evals_per_step": b_ev / args.steps, "clocks": clocks}
+            "evals_per_step": b_ev / args.steps, "clocks": clocks,
+            # one CUDA graph per step: queue reset, phase-0 seeding, the persistent kernel
+            "gpu_launches": 3 * args.steps}
     print(json.dumps(line))
     return 0
 
@@ -293,7 +295,10 @@ def run_large(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "kernel": "mc_large_kernel (cluster local search)", "bytes_per_eval": B,
                          "peak_kind": peak_kind},
-            "best_fitness_last_step": float(fit[0]), "evals_per_step": ev / args.steps, "clocks": clocks}
+            "best_fitness_last_step": float(fit[0]), "evals_per_step": ev / args.steps, "clocks": clocks,
+            # per step (one iteration): the slot-order reset; zero counts, generate, recount and fitness
+            # for each of the two generations; two cluster local searches; merge and survivor sorts
+            "gpu_launches": args.steps * 13}
     print(json.dumps(line))
     return 0
 
