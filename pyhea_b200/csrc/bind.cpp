@@ -5,7 +5,7 @@
 //                               weight, target_sro) -> (list[list[int]], list[float])
 //   cuda_available() -> bool
 //   run_local_parallel_hcs(...)  (the CPU engine, bind.cpp:7-46) is not part of
-//                               this build and raises RuntimeError
+//                               this module and raises RuntimeError
 // It calls the C ABI of libhea_cuda.so (include/hea_cuda.h) and nothing else;
 // the GIL is released while the search runs.
 #include <pybind11/numpy.h>
@@ -180,5 +180,5 @@ PYBIND11_MODULE(accelerate, m)
                 "this accelerate module is the B200 GPU engine; the CPU engine (device: cpu) is not part of it. "
                 "Use run_local_parallel_hcs_cuda (device: gpu).");
         },
-        "Not provided by this build: the CPU engine of pyhea.cpp.accelerate.");
+        "Not provided by this module: the CPU engine of pyhea.cpp.accelerate.");
 }
