@@ -566,7 +566,10 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
 {
     constexpr int S = L::S, NC = S * T * T, NCP = mc_ncount_pad(NC);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    int32_t *cnt = cnt_all + warp * NCP;  // this warp's copy of the counts
+    // kHist: one shared copy of the counts, updated by the whole block on an
+    // accept (the barrier after the histogram update publishes both); the
+    // gather form keeps one copy per warp so an accept needs no barrier
+    int32_t *cnt = kHist ? cnt_all : cnt_all + warp * NCP;
     int miss = rs.miss0;
     int64_t round = rs.round0, accepts = 0, evals = 0;
     bool yielded = false;
@@ -643,7 +646,7 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
             const int a = w.ab & 0xFF, b = (w.ab >> 8) & 0xFF;
             occ5[w.s1] = (uint8_t)(5 * b);  // same bytes from every thread
             occ5[w.s2] = (uint8_t)(5 * a);
-            for (int x = lane; x < NC; x += 32) {
+            for (int x = kHist ? tid : lane; x < NC; x += kHist ? blockDim.x : 32) {
                 const int k = x / (T * T), i = (x / T) % T, j = x % T;
                 const uint32_t h1 = w.h1[k], h2 = w.h2[k];
                 const int m = (w.m >> (8 * k)) & 0xFF;
@@ -653,7 +656,12 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
                                (j == a ? m : 0);
                 cnt[x] += ((i == a) - (i == b)) * uj + ((j == a) - (j == b)) * ui;
             }
-            __syncwarp();
+            if constexpr (kHist) {
+                update_hist<L>(c, nbor, hist, w.s1, w.s2, a, b);
+                __syncthreads();  // next round's proposals read the updated counts and histograms
+            } else {
+                __syncwarp();
+            }
             if (tr.records && warp == 0 && accepts < tr.cap) {
                 if (lane == 0) {
                     AcceptRecord r;
@@ -668,10 +676,6 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
                     int32_t *dst = tr.counts + accepts * NC;
                     for (int x = lane; x < NC; x += 32) dst[x] = cnt[x];
                 }
-            }
-            if constexpr (kHist) {
-                update_hist<L>(c, nbor, hist, w.s1, w.s2, a, b);
-                __syncthreads();  // next round's proposals read the updated histograms
             }
             cur = xf;
             miss = 0;
