@@ -358,17 +358,20 @@ __device__ __forceinline__ bool draw_pair(const SearchConst &c, uint32_t stream,
 // Lexicographic (f2, task) minimum: the lowest task wins ties.
 __device__ __forceinline__ bool better(double f, int q, double bf, int bq) { return f < bf || (f == bf && q < bq); }
 
+// The warp's lexicographic (f, q) minimum in every lane, q >= 0.  f is an f2
+// (>= +0, or +inf for no proposal): such doubles order like their bit
+// patterns, so three 32-bit warp reductions (high word, low word among the
+// lanes holding the minimal high word, task among the lanes holding the
+// minimal f) give the exact minimum.
 __device__ __forceinline__ void warp_argmin(double &f, int &q)
 {
-#pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        const double of = __shfl_xor_sync(0xFFFFFFFFu, f, o);
-        const int oq = __shfl_xor_sync(0xFFFFFFFFu, q, o);
-        if (better(of, oq, f, q)) {
-            f = of;
-            q = oq;
-        }
-    }
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(f);
+    const uint32_t hi = (uint32_t)(bits >> 32), lo = (uint32_t)bits;
+    const uint32_t mhi = __reduce_min_sync(0xFFFFFFFFu, hi);
+    const uint32_t mlo = __reduce_min_sync(0xFFFFFFFFu, hi == mhi ? lo : 0xFFFFFFFFu);
+    const uint32_t mq = __reduce_min_sync(0xFFFFFFFFu, (hi == mhi && lo == mlo) ? (uint32_t)q : 0xFFFFFFFFu);
+    f = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+    q = (int)mq;
 }
 
 // Exact site histogram (5-bit field per species) from the recount's 10-bit
@@ -629,18 +632,11 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
         // every warp reduces the records of all warps
         double xf = lane < nwarps ? rr[lane].f2 : inf_d();
         int xq = lane < nwarps ? rr[lane].task : 0x7FFFFFFF;
-        int xw = lane;
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            const double of = __shfl_xor_sync(0xFFFFFFFFu, xf, o);
-            const int oq = __shfl_xor_sync(0xFFFFFFFFu, xq, o);
-            const int ow = __shfl_xor_sync(0xFFFFFFFFu, xw, o);
-            if (better(of, oq, xf, xq)) {
-                xf = of;
-                xq = oq;
-                xw = ow;
-            }
-        }
+        const double own_f = xf;
+        const int own_q = xq;
+        warp_argmin(xf, xq);
+        // the record holding the minimum (tasks of finite records are distinct)
+        const int xw = __ffs(__ballot_sync(0xFFFFFFFFu, own_f == xf && own_q == xq)) - 1;
         if (xf < cur) {
             const SwapRecord &w = rr[xw];
             const int a = w.ab & 0xFF, b = (w.ab >> 8) & 0xFF;
