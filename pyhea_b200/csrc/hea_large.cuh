@@ -122,7 +122,9 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
     const int sol = blockIdx.x / csize;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     int32_t *cnt_all = reinterpret_cast<int32_t *>(smem);
-    int32_t *cnt = cnt_all + warp * NCP;
+    // with site histograms an accept ends with a cluster barrier anyway, so one shared copy of the
+    // counts, updated by the whole CTA, replaces the per-warp copies
+    int32_t *cnt = HEA_SITE_HIST ? cnt_all : cnt_all + warp * NCP;
     SwapRecord *rec = reinterpret_cast<SwapRecord *>(cnt_all + nwarps * NCP);  // [2][nwarps]
     SwapRecord *cta_rec = rec + 2 * nwarps;                                      // [2]: this CTA's best
 
@@ -137,7 +139,7 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
     const int qpart = (g.tasks + csize - 1) / csize, qlo = rank * qpart, qhi = min(g.tasks, qlo + qpart);
 
     for (int s = lo + tid; s < hi; s += blockDim.x) row[s] = (uint8_t)(5 * row[s]);
-    for (int x = lane; x < NC; x += 32) cnt[x] = gcnt[x];
+    for (int x = HEA_SITE_HIST ? tid : lane; x < NC; x += HEA_SITE_HIST ? blockDim.x : 32) cnt[x] = gcnt[x];
     cluster.sync();
 
     double cur = g.f2[slot];
@@ -195,47 +197,31 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
         if (warp == 0) {
             double xf = lane < nwarps ? rr[lane].f2 : inf_d();
             int xq = lane < nwarps ? rr[lane].task : 0x7FFFFFFF;
-            int xw = lane;
-#pragma unroll
-            for (int o = 16; o; o >>= 1) {
-                const double of = __shfl_xor_sync(0xFFFFFFFFu, xf, o);
-                const int oq = __shfl_xor_sync(0xFFFFFFFFu, xq, o);
-                const int ow = __shfl_xor_sync(0xFFFFFFFFu, xw, o);
-                if (better(of, oq, xf, xq)) {
-                    xf = of;
-                    xq = oq;
-                    xw = ow;
-                }
-            }
+            const double own_f = xf;
+            const int own_q = xq;
+            warp_argmin(xf, xq);
+            const int xw = __ffs(__ballot_sync(0xFFFFFFFFu, own_f == xf && own_q == xq)) - 1;
             if (lane == 0) cta_rec[round & 1] = rr[xw];
         }
         cluster.sync();
         // every warp reduces the cluster's records
         double xf = inf_d();
-        int xq = 0x7FFFFFFF, xr = 0;
+        int xq = 0x7FFFFFFF;
         if (lane < csize) {
             const SwapRecord *remote = cluster.map_shared_rank(&cta_rec[round & 1], lane);
             xf = remote->f2;
             xq = remote->task;
-            xr = lane;
         }
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            const double of = __shfl_xor_sync(0xFFFFFFFFu, xf, o);
-            const int oq = __shfl_xor_sync(0xFFFFFFFFu, xq, o);
-            const int orr = __shfl_xor_sync(0xFFFFFFFFu, xr, o);
-            if (better(of, oq, xf, xq)) {
-                xf = of;
-                xq = oq;
-                xr = orr;
-            }
-        }
+        const double own_f = xf;
+        const int own_q = xq;
+        warp_argmin(xf, xq);
+        const int xr = __ffs(__ballot_sync(0xFFFFFFFFu, own_f == xf && own_q == xq)) - 1;
         if (xf < cur) {
             const SwapRecord w = *cluster.map_shared_rank(&cta_rec[round & 1], xr);
             const int a = w.ab & 0xFF, b = (w.ab >> 8) & 0xFF;
             row[w.s1] = (uint8_t)(5 * b);  // every CTA writes the swap itself
             row[w.s2] = (uint8_t)(5 * a);
-            for (int x = lane; x < NC; x += 32) {
+            for (int x = HEA_SITE_HIST ? tid : lane; x < NC; x += HEA_SITE_HIST ? blockDim.x : 32) {
                 const int k = x / (T * T), i = (x / T) % T, j = x % T;
                 const uint32_t h1 = w.h1[k], h2 = w.h2[k];
                 const int m = (w.m >> (8 * k)) & 0xFF;
@@ -245,7 +231,12 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
                                (j == a ? m : 0);
                 cnt[x] += ((i == a) - (i == b)) * uj + ((j == a) - (j == b)) * ui;
             }
-            __syncwarp();
+            if constexpr (HEA_SITE_HIST != 0) {
+                if (rank == 0) update_hist<L>(c, g.nbor, hist, w.s1, w.s2, a, b);
+                cluster.sync();  // the cluster's next proposals read the updated counts and histograms
+            } else {
+                __syncwarp();
+            }
             if (g.trace && rank == 0 && warp == 0 && accepts < g.trace_cap) {
                 if (lane == 0) {
                     AcceptRecord r;
@@ -260,10 +251,6 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
                     int32_t *dst = g.trace_counts + ((size_t)sol * g.trace_cap + accepts) * NC;
                     for (int x = lane; x < NC; x += 32) dst[x] = cnt[x];
                 }
-            }
-            if constexpr (HEA_SITE_HIST != 0) {
-                if (rank == 0) update_hist<L>(c, g.nbor, hist, w.s1, w.s2, a, b);
-                cluster.sync();  // the cluster's next proposals read the updated histograms
             }
             cur = xf;
             miss = 0;
