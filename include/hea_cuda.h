@@ -129,6 +129,11 @@ int hea_batch_run(hea_batch *batch, const uint64_t *seeds, hea_stats *stats);
 int hea_batch_read(hea_batch *batch, int32_t index, uint8_t *out_occ, double *out_fitness);
 /* Milliseconds from the start of the last run to each structure's final sort (device clock). */
 int hea_batch_finish_times(hea_batch *batch, double *out_ms);
+/* Autotuner of the batch's launch: times full runs (with the current seeds) for
+ * occupancy kept in HBM or staged in shared memory where it fits, at the
+ * kernel's resident CTAs per SM or one fewer, and keeps the fastest.  Results
+ * do not depend on the choice.  Outputs may be NULL. */
+int hea_batch_autotune(hea_batch *batch, int32_t *out_hbm_all, int32_t *out_ctas_per_sm);
 void hea_batch_destroy(hea_batch *batch);
 
 /*

@@ -114,6 +114,7 @@ def _declare(lib):
         "hea_batch_run": (_i32, [ctypes.c_void_p, _P(_u64), _P(Stats)]),
         "hea_batch_read": (_i32, [ctypes.c_void_p, _i32, _P(_u8), _P(_f64)]),
         "hea_batch_finish_times": (_i32, [ctypes.c_void_p, _P(_f64)]),
+        "hea_batch_autotune": (_i32, [ctypes.c_void_p, _P(_i32), _P(_i32)]),
         "hea_batch_destroy": (None, [ctypes.c_void_p]),
         "hea_server_create": (_i32, [_P(_ServerConfig), _P(ctypes.c_void_p)]),
         "hea_server_submit": (_i32, [ctypes.c_void_p, _P(_Problem), _P(_Params), _f64, _i32, _P(_i64)]),
@@ -265,6 +266,13 @@ class Batch:
         fit = np.empty(self.P[index], dtype=np.float64)
         _check(lib.hea_batch_read(self._h, int(index), _ptr(occ, _u8), _ptr(fit, _f64)))
         return occ, fit
+
+    def autotune(self):
+        """Time the launch configurations on full runs (current seeds) and keep the fastest;
+        returns {"hbm_all": 0|1, "ctas_per_sm": n}.  Results do not depend on it."""
+        h, c = _i32(), _i32()
+        _check(lib.hea_batch_autotune(self._h, ctypes.byref(h), ctypes.byref(c)))
+        return {"hbm_all": h.value, "ctas_per_sm": c.value}
 
     def finish_times(self):
         """Milliseconds from the start of the last run to each structure's end."""

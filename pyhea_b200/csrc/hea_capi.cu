@@ -1427,6 +1427,13 @@ extern "C" int hea_recount_noalloc(const hea_problem *problem, int32_t count, co
 // ---------------------------------------------------------------------------
 #include "hea_batch.cuh"
 
+namespace {
+struct BatchLevels {
+    unsigned long long total[kBatchLevels], base[kBatchLevels];
+};
+}  // namespace
+using BatchLevels_ = BatchLevels;
+
 struct hea_batch {
     int count = 0;
     std::vector<DeviceTables *> tables;
@@ -1446,8 +1453,11 @@ struct hea_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     uint8_t *out_occ = nullptr;
     double *out_f2 = nullptr;
+    BatchLevels_ *lv = nullptr;  // queue layout of the graph's reset kernel
+    int hbm_all = 1, ctas_per_sm = HEA_BATCH_MIN_BLOCKS;  // current launch configuration
     ~hea_batch()
     {
+        delete lv;
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         for (void *p : buffers) cudaFree(p);
@@ -1459,10 +1469,6 @@ struct hea_batch {
 };
 
 namespace {
-
-struct BatchLevels {
-    unsigned long long total[kBatchLevels], base[kBatchLevels];
-};
 
 __global__ void batch_reset_kernel(BatchCtl *ctl, BatchJob *jobs, unsigned long long njobs, BatchLevels lv,
                                    unsigned long long limit_ns)
@@ -1513,7 +1519,7 @@ size_t batch_job_smem(int occ_stride, int64_t ncount, int nwarps, bool hbm)
 
 // Dynamic shared memory per CTA that still lets HEA_BATCH_MIN_BLOCKS batch CTAs
 // share an SM.
-int batch_smem_budget(size_t *out)
+int batch_smem_budget(size_t *out, int ctas_per_sm = HEA_BATCH_MIN_BLOCKS)
 {
     cudaFuncAttributes a;
     int dev = 0, per_sm = 0, reserved = 0;
@@ -1521,10 +1527,58 @@ int batch_smem_budget(size_t *out)
     HEA_CUDA(cudaGetDevice(&dev));
     HEA_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
     HEA_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
-    long long b = (long long)per_sm / HEA_BATCH_MIN_BLOCKS - reserved - (long long)a.sharedSizeBytes;
+    long long b = (long long)per_sm / ctas_per_sm - reserved - (long long)a.sharedSizeBytes;
     b &= ~127ll;
     const long long lim = (long long)smem_limit() - (long long)a.sharedSizeBytes;
     *out = (size_t)std::max(0ll, std::min(b, lim));
+    return HEA_OK;
+}
+
+// Launch configuration of a batch: occupancy placement (hbm_all: every
+// structure's occupancy in HBM; otherwise in shared memory where the per-CTA
+// budget of ctas_per_sm CTAs per SM allows) and resident CTAs per SM; then the
+// run is captured again as a CUDA graph.  Results do not depend on it.
+int batch_configure(hea_batch *b, int hbm_all, int ctas_per_sm)
+{
+    const int nwarps = b->block / 32;
+    size_t budget = 0;
+    HEA_TRY(batch_smem_budget(&budget, ctas_per_sm));
+    size_t smem = 0;
+    for (int i = 0; i < b->count; ++i) {
+        BatchStruct &d = b->h_structs[i];
+        const int64_t ncount = b->tables[i]->ncount;
+        d.hbm = (hbm_all || batch_job_smem(d.c.occ_stride, ncount, nwarps, false) > budget) ? 1 : 0;
+        smem = std::max(smem, batch_job_smem(d.c.occ_stride, ncount, nwarps, d.hbm != 0));
+    }
+    cudaFuncAttributes a;
+    HEA_CUDA(cudaFuncGetAttributes(&a, batch_kernel));
+    if (smem + a.sharedSizeBytes > (size_t)smem_limit())
+        return fail(HEA_ERR_UNSUPPORTED, "the largest structure needs %zu bytes of shared memory, above %d", smem,
+                    smem_limit() - (int)a.sharedSizeBytes);
+    int per_sm = 0, sms = 0, dev = 0;
+    HEA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, b->block, smem));
+    HEA_CUDA(cudaGetDevice(&dev));
+    HEA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    per_sm = std::min(per_sm, ctas_per_sm);
+    if (per_sm < 1) return fail(HEA_ERR_UNSUPPORTED, "batch kernel does not fit on an SM");
+    b->smem = smem;
+    b->grid = per_sm * sms;
+    b->hbm_all = hbm_all;
+    b->ctas_per_sm = per_sm;
+    HEA_CUDA(cudaStreamSynchronize(b->stream));
+    HEA_CUDA(cudaMemcpy(b->d_structs, b->h_structs.data(), sizeof(BatchStruct) * b->count, cudaMemcpyHostToDevice));
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    // the run as one CUDA graph: reset the queue, seed phase 0, persistent kernel
+    HEA_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    batch_reset_kernel<<<64, 256, 0, b->stream>>>(b->d_ctl, b->d_jobs, b->total_jobs, *b->lv, 60ull * 1000000000ull);
+    batch_seed_kernel<<<b->count, 256, 0, b->stream>>>(b->d_structs, nullptr, b->d_states, b->d_jobs, b->d_ctl);
+    batch_kernel<<<b->grid, b->block, b->smem, b->stream>>>(b->d_structs, b->d_states, b->d_jobs, b->d_ctl,
+                                                            b->d_finish);
+    HEA_CUDA(cudaStreamEndCapture(b->stream, &b->graph));
+    HEA_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
     return HEA_OK;
 }
 
@@ -1541,7 +1595,6 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
     if (!b) return fail(HEA_ERR_NOMEM, "out of host memory");
     b->count = count;
     int rc = HEA_OK;
-    const int nwarps = b->block / 32;
     for (int i = 0; i < count && rc == HEA_OK; ++i) {
         rc = validate_params(&params[i]);
         if (rc != HEA_OK) break;
@@ -1583,18 +1636,6 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
         b->h_structs.push_back(d);
         b->total_jobs += d.I > 0 ? (unsigned long long)P * (2 * d.I + 1) : (unsigned long long)P;
     }
-    // Occupancy in HBM: with site-histogram scoring a search reads it only for
-    // its draws, and small shared memory leaves room for more CTAs per SM and
-    // a larger L1 (measured faster than staging rows in shared memory).
-    // Without histograms, in shared memory while the per-SM budget allows.
-    size_t budget = 0;
-    if (rc == HEA_OK) rc = batch_smem_budget(&budget);
-    for (int i = 0; rc == HEA_OK && i < count; ++i) {
-        BatchStruct &d = b->h_structs[i];
-        const int64_t ncount = b->tables[i]->ncount;
-        d.hbm = (HEA_SITE_HIST || batch_job_smem(d.c.occ_stride, ncount, nwarps, false) > budget) ? 1 : 0;
-        b->smem = std::max(b->smem, batch_job_smem(d.c.occ_stride, ncount, nwarps, d.hbm != 0));
-    }
     // priority levels: structures ranked by work, largest first
     BatchLevels lv{};
     if (rc == HEA_OK) {
@@ -1623,42 +1664,21 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
     if (rc == HEA_OK) rc = batch_alloc(b, &b->out_occ, max_out);
     if (rc == HEA_OK) rc = batch_alloc(b, &b->out_f2, sizeof(double) * 65536);
     if (rc == HEA_OK) {
-        cudaFuncAttributes a;
-        if (cudaFuncGetAttributes(&a, batch_kernel) != cudaSuccess)
-            rc = fail(HEA_ERR_CUDA, "cannot query the batch kernel");
-        else if (b->smem + a.sharedSizeBytes > (size_t)smem_limit())
-            rc = fail(HEA_ERR_UNSUPPORTED, "the largest structure needs %zu bytes of shared memory, above %d", b->smem,
-                      smem_limit() - (int)a.sharedSizeBytes);
-    }
-    if (rc == HEA_OK) {
-        cudaError_t e = allow_max_smem(batch_kernel);
-        int per_sm = 0, sms = 0, dev = 0;
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel, b->block, b->smem);
-        if (e == cudaSuccess) e = cudaGetDevice(&dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e != cudaSuccess) rc = fail(HEA_ERR_CUDA, "batch kernel set-up failed: %s", cudaGetErrorString(e));
-        else if (per_sm < 1) rc = fail(HEA_ERR_UNSUPPORTED, "batch kernel does not fit on an SM");
-        b->grid = per_sm * sms;
+        b->lv = new (std::nothrow) BatchLevels(lv);
+        if (!b->lv) rc = fail(HEA_ERR_NOMEM, "out of host memory");
     }
     if (rc == HEA_OK) {
         cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
         if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
-        if (e == cudaSuccess)
-            e = cudaMemcpy(b->d_structs, b->h_structs.data(), sizeof(BatchStruct) * count, cudaMemcpyHostToDevice);
-        // the run as one CUDA graph: reset the queue, seed phase 0, persistent kernel
-        if (e == cudaSuccess) e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
-        if (e == cudaSuccess) {
-            batch_reset_kernel<<<64, 256, 0, b->stream>>>(b->d_ctl, b->d_jobs, b->total_jobs, lv, 60ull * 1000000000ull);
-            batch_seed_kernel<<<count, 256, 0, b->stream>>>(b->d_structs, nullptr, b->d_states, b->d_jobs, b->d_ctl);
-            batch_kernel<<<b->grid, b->block, b->smem, b->stream>>>(b->d_structs, b->d_states, b->d_jobs, b->d_ctl,
-                                                                    b->d_finish);
-            cudaError_t e2 = cudaStreamEndCapture(b->stream, &b->graph);
-            e = e2;
-        }
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
-        if (e != cudaSuccess) rc = fail(HEA_ERR_CUDA, "batch graph set-up failed: %s", cudaGetErrorString(e));
+        if (e == cudaSuccess) e = allow_max_smem(batch_kernel);
+        if (e != cudaSuccess) rc = fail(HEA_ERR_CUDA, "batch set-up failed: %s", cudaGetErrorString(e));
     }
+    // Occupancy in HBM by default: with site-histogram scoring a search reads it
+    // only for its draws, and small shared memory leaves room for more CTAs per
+    // SM and a larger L1 (measured faster on the mixed batch; hea_batch_autotune
+    // compares the alternatives on the batch at hand).
+    if (rc == HEA_OK) rc = batch_configure(b, HEA_SITE_HIST ? 1 : 0, HEA_BATCH_MIN_BLOCKS);
     if (rc != HEA_OK) {
         delete b;
         return rc;
@@ -1700,6 +1720,38 @@ int hea_batch_run(hea_batch *b, const uint64_t *seeds, hea_stats *stats)
         stats->mc_ms = ms;
         stats->mc_launches = 1;
     }
+    return HEA_OK;
+}
+
+int hea_batch_autotune(hea_batch *b, int32_t *out_hbm_all, int32_t *out_ctas_per_sm)
+{
+    if (!b) return fail(HEA_ERR_INVALID, "batch is NULL");
+    struct Cand {
+        int hbm_all, ctas;
+    };
+    // occupancy in HBM or in shared memory where it fits, at the kernel's CTAs per SM or one fewer
+    std::vector<Cand> cands;
+    for (int hbm_all : {1, 0})
+        for (int ctas : {HEA_BATCH_MIN_BLOCKS, HEA_BATCH_MIN_BLOCKS - 1})
+            if (ctas >= 1) cands.push_back(Cand{hbm_all, ctas});
+    double best_rate = -1.0;
+    Cand best = cands[0];
+    for (const Cand &cd : cands) {
+        const int rc = batch_configure(b, cd.hbm_all, cd.ctas);
+        if (rc == HEA_ERR_UNSUPPORTED) continue;  // this placement does not fit
+        HEA_TRY(rc);
+        hea_stats st{};
+        HEA_TRY(hea_batch_run(b, nullptr, &st));  // warm-up
+        HEA_TRY(hea_batch_run(b, nullptr, &st));
+        const double rate = st.gpu_ms > 0 ? st.evals / st.gpu_ms : 0.0;
+        if (rate > best_rate) {
+            best_rate = rate;
+            best = cd;
+        }
+    }
+    HEA_TRY(batch_configure(b, best.hbm_all, best.ctas));
+    if (out_hbm_all) *out_hbm_all = b->hbm_all;
+    if (out_ctas_per_sm) *out_ctas_per_sm = b->ctas_per_sm;
     return HEA_OK;
 }
 

@@ -68,3 +68,21 @@ def test_batch_matches_oracle_on_one_structure():
     np.testing.assert_array_equal(occ, wocc)
     np.testing.assert_array_equal(fit, np.sqrt(wf2))
     b.close()
+
+
+def test_autotuned_batch_gives_the_same_results():
+    """The batch autotuner only changes where occupancies live and how many CTAs share an SM."""
+    items = mixed_structures(4, 5)
+    seeds = [77 + 3 * i for i in range(len(items))]
+    b = hb.Batch([p for p, _ in items], [q for _, q in items])
+    b.run(seeds)
+    choice = b.autotune()
+    assert choice["hbm_all"] in (0, 1) and 1 <= choice["ctas_per_sm"] <= 3
+    b.run(seeds)
+    for i, (pb, q) in enumerate(items):
+        occ, fit = b.read(i)
+        pocc, pfit, _ = hb.search(pb, q["num_solutions"], q["total_iter"], q["parallel_task"], q["converge_depth"],
+                                  seed=seeds[i])
+        np.testing.assert_array_equal(occ, pocc, err_msg=f"structure {i}")
+        np.testing.assert_array_equal(fit, pfit, err_msg=f"structure {i}")
+    b.close()
