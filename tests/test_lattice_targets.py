@@ -84,3 +84,22 @@ def test_weighted_error_matches_oracle_fitness(golden_engine, golden_nbor):
     C = pr.recount(case["occ"][0].astype(np.uint8))
     f = sro.weighted_sro_error(C, case["shell_size"], case["species"], case["weight"], case["target"])
     assert abs(f - case["fitness"][0]) < 1e-12 * case["fitness"][0]
+
+
+def test_alpha_matches_reference_gamma(golden_engine, golden_nbor):
+    """alpha from the oracle's integer counts equals 1 - gamma/(c_i c_j) with the
+    reference engine's own gamma (accelerate.cpp:370-399, :171)."""
+    from conftest import engine_case_problem
+    from oracle import hea_oracle as ho
+
+    for name in ("fcc4_t4_s3", "bcc4_t3_s2", "bcc4_t6_s3"):
+        case = golden_engine[name]
+        pr = engine_case_problem(case, golden_nbor, ho)
+        sp = np.asarray(case["species"], dtype=np.float64)
+        c = sp / sp.sum()
+        for p in range(len(case["occ"])):
+            C = pr.recount(case["occ"][p].astype(np.uint8))
+            a = sro.alpha_from_counts(C, case["shell_size"], case["species"])
+            gamma = np.moveaxis(np.asarray(case["gamma"][p]), -1, 0)  # [T][T][S] -> [S][T][T]
+            ref_alpha = 1.0 - gamma / np.outer(c, c)[None]
+            np.testing.assert_allclose(a, ref_alpha, rtol=0, atol=1e-12)
