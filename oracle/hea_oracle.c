@@ -80,6 +80,18 @@ static int bounded(uint32_t x, uint32_t n, uint32_t thresh, uint32_t *v)
 
 uint32_t hea_oracle_reject_threshold(uint32_t n) { return (uint32_t)(0u - n) % n; }
 
+/* The same on a 16-bit word h (n <= 2^16): accept iff low16(h n) >= 2^16 mod n. */
+static int bounded16(uint32_t h, uint32_t n, uint32_t thresh, uint32_t *v)
+{
+    uint32_t m = h * n;
+    if ((m & 0xFFFFu) < thresh) return 0;
+    *v = m >> 16;
+    return 1;
+}
+
+/* 16-bit draws when n <= 2^16 and at most 1/16 of the 16-bit words are rejected. */
+int hea_oracle_use_draw16(uint32_t n) { return n <= 65536u && (65536u % n) <= 4096u; }
+
 /*
  * Draw the swap pair for (task, round) of one search stream.  Mirrors the
  * redraw loop at accelerate.cpp:649-655: both sites are redrawn until their
@@ -87,12 +99,30 @@ uint32_t hea_oracle_reject_threshold(uint32_t n) { return (uint32_t)(0u - n) % n
  * two attempts, (x0, x1) and then (x2, x3); an attempt is valid when both
  * bounded draws accept and the two species differ.  Returns the index of the
  * attempt used (2c or 2c+1), or -1 when HEA_ORACLE_MAX_CALLS calls found none.
+ * With 16-bit draws (hea_oracle_use_draw16), call c carries four attempts:
+ * attempt j takes the low and the high half of word x_j (index 4c + j).
  */
 #define HEA_ORACLE_MAX_CALLS (1u << 19)
 int64_t hea_oracle_draw_pair(const uint32_t key[2], uint32_t stream, uint32_t round, uint32_t task,
                              const uint8_t *occ, uint32_t n, uint32_t *s1, uint32_t *s2)
 {
     uint32_t th = hea_oracle_reject_threshold(n);
+    if (hea_oracle_use_draw16(n)) {
+        uint32_t th16 = 65536u % n;
+        for (uint32_t c = 0; c < HEA_ORACLE_MAX_CALLS; ++c) {
+            uint32_t ctr[4] = {c, task, round, stream}, x[4];
+            hea_oracle_philox(ctr, key, x);
+            for (int j = 0; j < 4; ++j) {
+                uint32_t u, v;
+                if (bounded16(x[j] & 0xFFFFu, n, th16, &u) && bounded16(x[j] >> 16, n, th16, &v) && occ[u] != occ[v]) {
+                    *s1 = u;
+                    *s2 = v;
+                    return (int64_t)(4 * c + j);
+                }
+            }
+        }
+        return -1;
+    }
     for (uint32_t c = 0; c < HEA_ORACLE_MAX_CALLS; ++c) {
         uint32_t ctr[4] = {c, task, round, stream}, x[4];
         hea_oracle_philox(ctr, key, x);

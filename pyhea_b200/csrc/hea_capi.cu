@@ -560,6 +560,8 @@ void fill_const(const hea_problem *pb, uint64_t seed, SearchConst &c, PadGeom &g
     c.occ_stride = (N + 1 + 15) & ~15;  // room for the sentinel byte N in HBM rows too
     c.feistel_h = feistel_half_bits((uint32_t)N);
     c.reject_below = (uint32_t)(0u - (uint32_t)N) % (uint32_t)N;
+    c.draw16 = use_draw16((uint32_t)N) ? 1u : 0u;
+    c.reject16 = c.draw16 ? 65536u % (uint32_t)N : 0u;
     c.key0 = (uint32_t)seed;
     c.key1 = (uint32_t)(seed >> 32);
     c.prefix[0] = 0;

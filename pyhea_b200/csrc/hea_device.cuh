@@ -48,6 +48,18 @@ __device__ __forceinline__ bool bounded_draw(uint32_t x, uint32_t n, uint32_t re
     return x * n >= reject_below;
 }
 
+// The same on a 16-bit word h (n <= 2^16): accept iff low16(h n) >= 2^16 mod n; value high16(h n).
+__device__ __forceinline__ bool bounded_draw16(uint32_t h, uint32_t n, uint32_t reject16, uint32_t &v)
+{
+    const uint32_t m = h * n;
+    v = m >> 16;
+    return (m & 0xFFFFu) >= reject16;
+}
+
+// Whether proposals of a structure of n sites use 16-bit draws (four attempts
+// per Philox call): n <= 2^16 and at most 1/16 of the 16-bit words rejected.
+__host__ __device__ __forceinline__ bool use_draw16(uint32_t n) { return n <= 65536u && (65536u % n) <= 4096u; }
+
 // murmur3 finaliser, the Feistel round function.
 __host__ __device__ __forceinline__ uint32_t fmix32(uint32_t h)
 {

@@ -27,6 +27,8 @@ struct SearchConst {
     int32_t prefix[kMaxTypes + 1];  // species prefix sums
     int32_t num_sites, row4, occ_stride, num_types, num_shells, feistel_h;
     uint32_t reject_below, key0, key1;
+    uint32_t draw16;    // 1: 16-bit draws, four attempts per Philox call (use_draw16)
+    uint32_t reject16;  // 2^16 mod N
 };
 
 // Shell layout of the padded table, in int4 chunks per shell (0: shell absent).
@@ -333,11 +335,30 @@ __device__ __forceinline__ void update_hist(const SearchConst &c, const int4 *__
 }
 
 // Two attempts per Philox call: (x0, x1) then (x2, x3); valid when both draws
-// accept and the species differ (pyhea/cpp/accelerate.cpp:649-655).
+// accept and the species differ (pyhea/cpp/accelerate.cpp:649-655).  With
+// 16-bit draws (draw16), four attempts per call: attempt j takes the low and
+// the high half of word x_j.
 __device__ __forceinline__ bool draw_pair(const SearchConst &c, uint32_t stream, uint32_t round, uint32_t task,
                                           const uint8_t *occ5, uint32_t &s1, uint32_t &s2)
 {
     const uint32_t n = (uint32_t)c.num_sites;
+    if (c.draw16) {
+        for (uint32_t call = 0; call < kPhiloxCallsPerDraw; ++call) {
+            const u32x4 x = philox4x32_10(u32x4{call, task, round, stream}, c.key0, c.key1);
+            const uint32_t w[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                uint32_t u, v;
+                if (bounded_draw16(w[j] & 0xFFFFu, n, c.reject16, u) && bounded_draw16(w[j] >> 16, n, c.reject16, v) &&
+                    occ5[u] != occ5[v]) {
+                    s1 = u;
+                    s2 = v;
+                    return true;
+                }
+            }
+        }
+        return false;
+    }
     for (uint32_t call = 0; call < kPhiloxCallsPerDraw; ++call) {
         const u32x4 x = philox4x32_10(u32x4{call, task, round, stream}, c.key0, c.key1);
         uint32_t u, v;

@@ -1,5 +1,7 @@
 """The CPU restatement (oracle/) pinned against the reference engine and its
 published primitives; CPU only."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -139,3 +141,24 @@ def test_hcs_sorted_deterministic_and_improving():
     init = [pr.f2(pr.recount(pr.generate(3, 0, s))) for s in range(4)]
     assert f2[0] < min(init)
     assert stats["evals"] > 0 and stats["accepts"] > 0
+
+
+def test_draw_modes():
+    """Structures of at most 2^16 sites with few rejected 16-bit words draw four
+    attempts per Philox call from 16-bit halves; the others two from 32-bit words."""
+    lib = ho.lib()
+    lib.hea_oracle_use_draw16.restype = ctypes.c_int
+    assert lib.hea_oracle_use_draw16(16000) == 1 and lib.hea_oracle_use_draw16(4000) == 1
+    assert lib.hea_oracle_use_draw16(35152) == 0 and lib.hea_oracle_use_draw16(65537) == 0
+    st = W.small_case(lattice=L.BCC, cell=26, species=(17576, 17576))
+    nbor, ss = st.neighbors()
+    pr = ho.Problem(nbor, ss, st.species, st.weight, st.target)
+    occ = pr.generate(2, 0, 0)
+    atts, seen = [], np.zeros(pr.num_sites)
+    for q in range(3000):
+        att, a, b = pr.draw_pair(9, 5, 0, q, occ)
+        assert att >= 0 and occ[a] != occ[b]
+        atts.append(att)
+        seen[a] += 1
+    assert max(atts) >= 2  # 32-bit mode: attempt 2 is the second Philox call
+    assert abs(seen[occ == 0].sum() / seen.sum() - 0.5) < 0.05

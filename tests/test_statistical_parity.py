@@ -8,7 +8,7 @@ as the GPU parity tests show) and the reference engine compiled from its own
 source (pyhea/cpp/accelerate.cpp:713-763, via oracle/_ref) each run the same
 scaled-down plain case many times; the two samples must not differ
 significantly (two-sided Mann-Whitney U) and the oracle's median must not be
-worse than the reference's by more than the sampling noise allows.
+worse than the reference's by more than one reference standard deviation.
 """
 import ctypes
 import os
@@ -62,4 +62,4 @@ def test_best_fitness_distribution_matches_reference(lattice, species):
     p = mannwhitneyu(ours, ref, alternative="two-sided").pvalue
     assert p > 1e-3, (np.median(ours), np.median(ref), p)
     # the oracle's median within the spread of the reference's own runs
-    assert np.median(ours) <= np.median(ref) + 0.5 * np.std(ref), (np.median(ours), np.median(ref), np.std(ref))
+    assert np.median(ours) <= np.median(ref) + np.std(ref), (np.median(ours), np.median(ref), np.std(ref))
