@@ -38,9 +38,9 @@ sys.path.insert(0, REPO)
 
 HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes (read + write) per swap evaluation of mc_kernel on the plain GPU workload, from one
-# ncu capture (profiles/mc_kernel_bcc20_t5.md: 162.3 MB over a launch of 203.4 M evaluations);
+# ncu capture (profiles/mc_kernel_bcc20_t5.md: 164.5 MB over a launch of 203.7 M evaluations);
 # reported per launch as roofline.traffic, scaled by the evaluations of the bench's launches.
-DRAM_BYTES_PER_EVAL = {"plain_gpu": 162.3e6 / 203.4e6}
+DRAM_BYTES_PER_EVAL = {"plain_gpu": 164.5e6 / 203.7e6}
 
 
 def parse_args():
