@@ -18,6 +18,10 @@ Fixtures written:
                      (pyhea/io/output.py:62-106) for seeded occupancies of FCC and
                      BCC cells (`python tests/golden/make_golden.py poscar` writes
                      only these)
+  lammps_conf.json   the reference's sample LAMMPS output (examples/conf.lmp, FCC
+                     10^3, 4 species): its occupancy in the reference lattice's site
+                     order, its lattice constant and the SHA-256 of its text
+                     (`python tests/golden/make_golden.py lammps` writes only this)
 
 The reference's Python modules import mpi4py, OVITO, dpdata and matplotlib at
 module level; none is needed by the two functions used here, so they are
@@ -64,12 +68,44 @@ def poscar_fixtures(lattice):
         write_poscar([int(x) for x in occ], lat, T, [f"E{t}" for t in range(T)], os.path.join(HERE, name))
 
 
+def lammps_fixture(lattice):
+    import hashlib
+
+    path = os.path.join(REFERENCE_ROOT, "examples", "conf.lmp")
+    text = open(path).read()
+    lines = text.splitlines()
+    n = int(lines[1].split()[0])
+    T = int(lines[2].split()[0])
+    edge = float(lines[3].split()[1])
+    cell = 10
+    a = edge / cell
+    lat = lattice([cell, cell, cell], "FCC", a, np.eye(3) * cell)
+    coords = np.asarray(lat.coords, dtype=np.float64)  # cell units, multiples of 1/2
+    assert len(coords) == n
+    site_of = {tuple(int(round(2 * v)) for v in xyz): i for i, xyz in enumerate(coords)}
+    occ = np.full(n, -1, dtype=np.int64)
+    start = lines.index("Atoms # atomic") + 2
+    for ln in lines[start:start + n]:
+        _, typ, x, y, z = ln.split()
+        occ[site_of[tuple(int(round(2 * float(v) / a)) for v in (x, y, z))]] = int(typ) - 1
+    assert occ.min() >= 0
+    fixture = {"source": "examples/conf.lmp", "lattice": "FCC", "cell": cell, "lattice_constant": a, "num_types": T,
+               "occupancy": "".join(str(int(t)) for t in occ), "sha256": hashlib.sha256(text.encode()).hexdigest(),
+               "head": lines[:11], "tail": lines[-2:]}
+    with open(os.path.join(HERE, "lammps_conf.json"), "w") as f:
+        json.dump(fixture, f, indent=1)
+
+
 def main():
     lattice, input_config = import_reference()
     if sys.argv[1:] == ["poscar"]:
         poscar_fixtures(lattice)
         return
+    if sys.argv[1:] == ["lammps"]:
+        lammps_fixture(lattice)
+        return
     poscar_fixtures(lattice)
+    lammps_fixture(lattice)
 
     # 1. neighbour lists
     nb = {}

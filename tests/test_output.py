@@ -1,5 +1,6 @@
-"""POSCAR writer against files written by the reference writer
-(pyhea/io/output.py:62-106, fixtures from tests/golden/make_golden.py)."""
+"""Structure writers against the reference's own output: POSCAR files written
+by the reference writer (pyhea/io/output.py:62-106) and the reference's sample
+LAMMPS output (examples/conf.lmp); fixtures from tests/golden/make_golden.py."""
 import os
 
 import numpy as np
@@ -32,3 +33,35 @@ def test_poscar_counts_and_grouping():
     assert labels == ["A", "B", "C"] and counts == [6, 4, 6]
     pos = output.site_coordinates(L.BCC, 2)
     np.testing.assert_array_equal(xyz, pos[np.argsort(occ, kind="stable")])
+
+
+def test_lammps_matches_reference_sample():
+    """Byte-identical to the reference's sample LAMMPS output (examples/conf.lmp,
+    fixture from tests/golden/make_golden.py lammps)."""
+    import hashlib
+    import json
+
+    fx = json.load(open(os.path.join(GOLDEN, "lammps_conf.json")))
+    occ = np.array([int(c) for c in fx["occupancy"]], dtype=np.uint8)
+    text = output.lammps_text(occ, L.FCC, fx["cell"], fx["lattice_constant"], fx["num_types"])
+    lines = text.splitlines()
+    assert lines[:11] == fx["head"] and lines[-2:] == fx["tail"]
+    assert hashlib.sha256(text.encode()).hexdigest() == fx["sha256"]
+
+
+def test_lammps_roundtrip_and_write_structure(tmp_path):
+    occ = np.random.default_rng(5).integers(0, 3, size=L.num_sites(L.BCC, 3))
+    edges, tilts, ids, types, xyz = output.read_lammps(output.lammps_text(occ, L.BCC, 3, 2.5, 3))
+    order = np.argsort(occ, kind="stable")
+    np.testing.assert_array_equal(edges, [7.5, 7.5, 7.5])
+    np.testing.assert_array_equal(tilts, [0.0, 0.0, 0.0])
+    np.testing.assert_array_equal(ids, np.arange(1, occ.size + 1))
+    np.testing.assert_array_equal(types, occ[order] + 1)
+    np.testing.assert_array_equal(xyz, output.site_coordinates(L.BCC, 3)[order] * 2.5)
+    # the reference writer's format names and file naming (pyhea/io/output.py:14-58)
+    p = output.write_structure(str(tmp_path / "best.vasp"), occ, L.BCC, 3, 2.5, 3)
+    assert p.endswith("best.vasp") and output.read_poscar(p)[3] == list(np.bincount(occ, minlength=3))
+    p = output.write_structure(str(tmp_path / "best.vasp"), occ, L.BCC, 3, 2.5, 3, output_format="lammps/lmp")
+    assert p.endswith("best.lmp") and open(p).read() == output.lammps_text(occ, L.BCC, 3, 2.5, 3)
+    with pytest.raises(ValueError):
+        output.write_structure(str(tmp_path / "x"), occ, L.BCC, 3, output_format="xyz")
