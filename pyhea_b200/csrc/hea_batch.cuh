@@ -287,6 +287,8 @@ __device__ __noinline__ JobEnd batch_job(const SearchConst &c, const BatchStruct
     const uint32_t call = job.kind == kJobMc2 ? (uint32_t)(2 * job.iter + 1) : (uint32_t)(2 * job.iter);
     const uint32_t stream = (call << 16) | (uint32_t)pos;
     const McResume rs{job.resume ? (int64_t)job.round0 : 0, job.resume ? job.miss0 : 0, deadline, d.tol2};
+    // the draws read the species from the occupancy: measured on the mixed batch, the histograms'
+    // species words (draw_pair_hist) were slower for every structure size
     const McTally t = mc_rounds<T, L, HEA_BATCH_AHEAD, true, HEA_SITE_HIST != 0>(
         c, d.nbor, occ5, cnt_all, rec, stream, cur, d.Q, d.D, d.max_rounds, McTrace{nullptr, nullptr, 0}, rs, hist,
         d.nbmask);

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(256) large_recount_kernel(const SearchConst c,
             }
             hk[k] = h - (uint32_t)c.pad[k];  // sentinel entries counted as species 0
         }
-        if (hs) hs[s] = make_uint4(hk[0], hk[1], hk[2], 0u);
+        if (hs) hs[s] = make_uint4(hk[0], hk[1], hk[2], (uint32_t)(5 * a));  // species word: 5*species
     }
     __syncthreads();
     int32_t *g = cnt + (size_t)slot * S * T * T;
@@ -156,19 +156,26 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
         for (int q0 = qlo + warp * 32; q0 < qhi; q0 += blockDim.x) {
             const int q = q0 + lane;
             uint32_t s1 = 0, s2 = 0;
-            const bool ok = q < qhi && draw_pair(c, stream, (uint32_t)round, (uint32_t)q, row, s1, s2);
+            uint4 hp = make_uint4(0u, 0u, 0u, 0u), hq = hp;
+            // with histograms the species come from their species words: one L2 round trip per attempt
+            const bool ok = q < qhi && (HEA_SITE_HIST != 0
+                                            ? draw_pair_hist(c, stream, (uint32_t)round, (uint32_t)q, hist, s1, s2, hp, hq)
+                                            : draw_pair(c, stream, (uint32_t)round, (uint32_t)q, row, s1, s2));
             __syncwarp();
             double f = inf_d();
             uint32_t h1[S], h2[S];
             int m[S], a = 0, b = 0;
             if (ok) {
                 ++evals;
-                a = row[s1] / 5;
-                b = row[s2] / 5;
-                if constexpr (HEA_SITE_HIST != 0)
-                    f = score_swap_hist<T, L>(c, g.nbor, hist, g.nbmask, cnt, s1, s2, a, b, h1, h2, m);
-                else
+                if constexpr (HEA_SITE_HIST != 0) {
+                    a = (int)hp.w / 5;
+                    b = (int)hq.w / 5;
+                    f = score_swap_hist<T, L>(c, g.nbor, hp, hq, g.nbmask, cnt, s1, s2, a, b, h1, h2, m);
+                } else {
+                    a = row[s1] / 5;
+                    b = row[s2] / 5;
                     f = score_swap<T, L>(c, g.nbor, row, cnt, s1, s2, a, b, h1, h2, m);
+                }
             }
             double wf = f;
             int wq = ok ? q : 0x7FFFFFFF;
@@ -232,7 +239,7 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
                 cnt[x] += ((i == a) - (i == b)) * uj + ((j == a) - (j == b)) * ui;
             }
             if constexpr (HEA_SITE_HIST != 0) {
-                if (rank == 0) update_hist<L>(c, g.nbor, hist, w.s1, w.s2, a, b);
+                if (rank == 0) update_hist<L, true>(c, g.nbor, hist, w.s1, w.s2, a, b);
                 cluster.sync();  // the cluster's next proposals read the updated counts and histograms
             } else {
                 __syncwarp();

@@ -272,15 +272,16 @@ __device__ __forceinline__ double score_swap(const SearchConst &c, const int4 *_
 // listed among s1's shell-k neighbours) needs the table.  nbmask has bit
 // (n - s + N - 1) set for every table entry n of every site s; a clear bit for
 // s2 - s1 proves m = 0 in every shell, a set bit sends the lane to count s2
-// in s1's row.  Loads go through L2: the accept step updates H with atomics.
+// in s1's row.  Loads of H go through L2: the accept step updates H with
+// atomics.
+// p = hist[s1] and q = hist[s2], already loaded.
 template <int T, class L>
-__device__ __forceinline__ double score_swap_hist(const SearchConst &c, const int4 *__restrict__ nbor,
-                                                  const uint4 *hist, const uint32_t *__restrict__ nbmask,
+__device__ __forceinline__ double score_swap_hist(const SearchConst &c, const int4 *__restrict__ nbor, const uint4 p,
+                                                  const uint4 q, const uint32_t *__restrict__ nbmask,
                                                   const int32_t *cnt, uint32_t s1, uint32_t s2, int a, int b,
                                                   uint32_t (&h1)[L::S], uint32_t (&h2)[L::S], int (&m)[L::S])
 {
     constexpr int S = L::S;
-    const uint4 p = __ldcg(hist + s1), q = __ldcg(hist + s2);
     const uint32_t d = s2 - s1 + (uint32_t)c.num_sites - 1u;
     const bool near = (__ldg(nbmask + (d >> 5)) >> (d & 31u)) & 1u;
     const uint32_t pv[3] = {p.x, p.y, p.z}, qv[3] = {q.x, q.y, q.z};
@@ -313,7 +314,10 @@ __device__ __forceinline__ double score_swap_hist(const SearchConst &c, const in
 // histograms of every neighbour listed in both rows (block-wide, atomics in
 // L2; the caller's barrier publishes them).  An entry n in shell k of s1's row
 // means s1 is in n's shell k as often, since tables are symmetric per shell.
-template <class L>
+// kSpeciesWord: also the species words of s1 and s2, which draw_pair_hist
+// reads; searches whose draws read the occupancy leave them at their recount
+// values.
+template <class L, bool kSpeciesWord>
 __device__ __forceinline__ void update_hist(const SearchConst &c, const int4 *__restrict__ nbor, uint4 *hist,
                                             uint32_t s1, uint32_t s2, int a, int b)
 {
@@ -332,14 +336,19 @@ __device__ __forceinline__ void update_hist(const SearchConst &c, const int4 *__
         uint32_t *h = reinterpret_cast<uint32_t *>(hist + n) + k;
         atomicAdd(h, first ? up : 0u - up);
     }
+    if (kSpeciesWord && threadIdx.x == 0) {
+        hist[s1].w = (uint32_t)(5 * b);
+        hist[s2].w = (uint32_t)(5 * a);
+    }
 }
 
 // Two attempts per Philox call: (x0, x1) then (x2, x3); valid when both draws
 // accept and the species differ (pyhea/cpp/accelerate.cpp:649-655).  With
 // 16-bit draws (draw16), four attempts per call: attempt j takes the low and
-// the high half of word x_j.
-__device__ __forceinline__ bool draw_pair(const SearchConst &c, uint32_t stream, uint32_t round, uint32_t task,
-                                          const uint8_t *occ5, uint32_t &s1, uint32_t &s2)
+// the high half of word x_j.  differ(u, v) reads the two sites' species.
+template <class Differ>
+__device__ __forceinline__ bool draw_pair_by(const SearchConst &c, uint32_t stream, uint32_t round, uint32_t task,
+                                             Differ &&differ, uint32_t &s1, uint32_t &s2)
 {
     const uint32_t n = (uint32_t)c.num_sites;
     if (c.draw16) {
@@ -350,7 +359,7 @@ __device__ __forceinline__ bool draw_pair(const SearchConst &c, uint32_t stream,
             for (int j = 0; j < 4; ++j) {
                 uint32_t u, v;
                 if (bounded_draw16(w[j] & 0xFFFFu, n, c.reject16, u) && bounded_draw16(w[j] >> 16, n, c.reject16, v) &&
-                    occ5[u] != occ5[v]) {
+                    differ(u, v)) {
                     s1 = u;
                     s2 = v;
                     return true;
@@ -362,18 +371,42 @@ __device__ __forceinline__ bool draw_pair(const SearchConst &c, uint32_t stream,
     for (uint32_t call = 0; call < kPhiloxCallsPerDraw; ++call) {
         const u32x4 x = philox4x32_10(u32x4{call, task, round, stream}, c.key0, c.key1);
         uint32_t u, v;
-        if (bounded_draw(x.x, n, c.reject_below, u) && bounded_draw(x.y, n, c.reject_below, v) && occ5[u] != occ5[v]) {
+        if (bounded_draw(x.x, n, c.reject_below, u) && bounded_draw(x.y, n, c.reject_below, v) && differ(u, v)) {
             s1 = u;
             s2 = v;
             return true;
         }
-        if (bounded_draw(x.z, n, c.reject_below, u) && bounded_draw(x.w, n, c.reject_below, v) && occ5[u] != occ5[v]) {
+        if (bounded_draw(x.z, n, c.reject_below, u) && bounded_draw(x.w, n, c.reject_below, v) && differ(u, v)) {
             s1 = u;
             s2 = v;
             return true;
         }
     }
     return false;
+}
+
+// Species from the occupancy (5*species bytes).
+__device__ __forceinline__ bool draw_pair(const SearchConst &c, uint32_t stream, uint32_t round, uint32_t task,
+                                          const uint8_t *occ5, uint32_t &s1, uint32_t &s2)
+{
+    return draw_pair_by(c, stream, round, task, [occ5](uint32_t u, uint32_t v) { return occ5[u] != occ5[v]; }, s1, s2);
+}
+
+// Species from the site histograms' species words (hist[s].w = 5*species):
+// for an occupancy in HBM this makes the two 16-byte L2 loads of an attempt
+// the only memory round trip of a proposal; p, q are the accepted pair's
+// histograms.
+__device__ __forceinline__ bool draw_pair_hist(const SearchConst &c, uint32_t stream, uint32_t round, uint32_t task,
+                                               const uint4 *hist, uint32_t &s1, uint32_t &s2, uint4 &p, uint4 &q)
+{
+    return draw_pair_by(
+        c, stream, round, task,
+        [hist, &p, &q](uint32_t u, uint32_t v) {
+            p = __ldcg(hist + u);
+            q = __ldcg(hist + v);
+            return p.w != q.w;
+        },
+        s1, s2);
 }
 
 // Lexicographic (f2, task) minimum: the lowest task wins ties.
@@ -409,8 +442,9 @@ __device__ __forceinline__ uint32_t pack_hist5(uint64_t h10, int pad)
 // ---------------------------------------------------------------------------
 // Block recount of the pair counts of the occupancy in shared memory.
 // With `hist`, also writes every site's histograms: hist[s] = {H_0, H_1, H_2,
-// 0}, H_k = sum over s's shell-k neighbours n of 1 << (5 species(n)) -- the
-// species histogram of the neighbourhood, one 5-bit field per species.
+// 5 species(s)}, H_k = sum over s's shell-k neighbours n of 1 << (5
+// species(n)) -- the species histogram of the neighbourhood, one 5-bit field
+// per species -- and the last word the site's own species (5*species).
 // Per-thread packed 10-bit accumulators [T][S], flushed to shared-memory bins
 // every 32 sites (32 sites * 28 entries < 1024).  Sentinel entries land in
 // field 0 and are removed at the end (pad_k * n_i per row i).
@@ -458,7 +492,7 @@ __device__ void block_recount(const SearchConst &c, const int4 *__restrict__ nbo
                 if (a5 == 5 * i) acc[i][k] += h;
             if (hist) hs[k] = pack_hist5<T>(h, c.pad[k]);
         }
-        if (hist) hist[s] = make_uint4(hs[0], hs[1], hs[2], 0u);
+        if (hist) hist[s] = make_uint4(hs[0], hs[1], hs[2], (uint32_t)a5);
         if (++since == 32) {
             flush();
             since = 0;
@@ -580,8 +614,10 @@ struct McResume {
 // copies in cnt_all).  Every thread returns the same f2/rounds/accepts; evals
 // is this thread's count.  No barrier at entry; one per round.  occ5 may be
 // shared or global memory; every thread writes the accepted swap's bytes
-// itself, so its own later loads see them either way.
-template <int T, class L, bool kAhead = false, bool kYield = false, bool kHist = false>
+// itself, so its own later loads see them either way.  kHist with kDrawHist:
+// the draws read the species from the histograms' species words (for an
+// occupancy in HBM), else from occ5.
+template <int T, class L, bool kAhead = false, bool kYield = false, bool kHist = false, bool kDrawHist = false>
 __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *__restrict__ nbor, uint8_t *occ5,
                                              int32_t *cnt_all, SwapRecord *rec, uint32_t stream, double cur,
                                              int tasks, int depth, int64_t max_rounds, McTrace tr,
@@ -609,19 +645,30 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
         for (int q0 = warp * 32; q0 < tasks; q0 += blockDim.x) {
             const int q = q0 + lane;
             uint32_t s1 = 0, s2 = 0;
-            const bool ok = q < tasks && draw_pair(c, stream, (uint32_t)round, (uint32_t)q, occ5, s1, s2);
+            uint4 hp = make_uint4(0u, 0u, 0u, 0u), hq = hp;
+            const bool ok = q < tasks && ((kHist && kDrawHist)
+                                              ? draw_pair_hist(c, stream, (uint32_t)round, (uint32_t)q, hist, s1, s2, hp, hq)
+                                              : draw_pair(c, stream, (uint32_t)round, (uint32_t)q, occ5, s1, s2));
             __syncwarp();  // lanes that needed more draws rejoin before scoring
             double f = inf_d();
             uint32_t h1[S], h2[S];
             int m[S], a = 0, b = 0;
             if (ok) {
                 ++evals;
-                a = occ5[s1] / 5;
-                b = occ5[s2] / 5;
-                if constexpr (kHist)
-                    f = score_swap_hist<T, L>(c, nbor, hist, nbmask, cnt, s1, s2, a, b, h1, h2, m);
-                else
+                if constexpr (kHist && kDrawHist) {
+                    a = (int)hp.w / 5;
+                    b = (int)hq.w / 5;
+                    f = score_swap_hist<T, L>(c, nbor, hp, hq, nbmask, cnt, s1, s2, a, b, h1, h2, m);
+                } else if constexpr (kHist) {
+                    a = occ5[s1] / 5;
+                    b = occ5[s2] / 5;
+                    f = score_swap_hist<T, L>(c, nbor, __ldcg(hist + s1), __ldcg(hist + s2), nbmask, cnt, s1, s2, a, b,
+                                              h1, h2, m);
+                } else {
+                    a = occ5[s1] / 5;
+                    b = occ5[s2] / 5;
                     f = score_swap<T, L, kAhead>(c, nbor, occ5, cnt, s1, s2, a, b, h1, h2, m);
+                }
             }
             double wf = f;
             int wq = ok ? q : 0x7FFFFFFF;
@@ -674,7 +721,7 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
                 cnt[x] += ((i == a) - (i == b)) * uj + ((j == a) - (j == b)) * ui;
             }
             if constexpr (kHist) {
-                update_hist<L>(c, nbor, hist, w.s1, w.s2, a, b);
+                update_hist<L, kDrawHist>(c, nbor, hist, w.s1, w.s2, a, b);
                 __syncthreads();  // next round's proposals read the updated counts and histograms
             } else {
                 __syncwarp();
