@@ -240,6 +240,18 @@ struct JobEnd {
 #ifndef HEA_BATCH_AHEAD
 #define HEA_BATCH_AHEAD true  // whole-row loads before use (the batch kernel has 128 registers per thread)
 #endif
+// The rounds of a job's local search in a call of their own: values the job
+// needs only before and after the search stay out of the loop's registers.
+template <int T, class L>
+__device__ __noinline__ McTally batch_search(const SearchConst &c, const BatchStruct &d, uint8_t *occ5,
+                                             int32_t *cnt_all, SwapRecord *rec, uint32_t stream, double cur,
+                                             const McResume rs, uint4 *hist)
+{
+    return mc_rounds<T, L, HEA_BATCH_AHEAD, true, HEA_SITE_HIST != 0>(
+        c, d.nbor, occ5, cnt_all, rec, stream, cur, d.Q, d.D, d.max_rounds, McTrace{nullptr, nullptr, 0}, rs, hist,
+        d.nbmask);
+}
+
 template <int T, class L>
 __device__ __noinline__ JobEnd batch_job(const SearchConst &c, const BatchStruct &d, const BatchJob &job,
                                          uint8_t *smem, unsigned long long *stats, unsigned long long *tally,
@@ -289,9 +301,7 @@ __device__ __noinline__ JobEnd batch_job(const SearchConst &c, const BatchStruct
     const McResume rs{job.resume ? (int64_t)job.round0 : 0, job.resume ? job.miss0 : 0, deadline, d.tol2};
     // the draws read the species from the occupancy: measured on the mixed batch, the histograms'
     // species words (draw_pair_hist) were slower for every structure size
-    const McTally t = mc_rounds<T, L, HEA_BATCH_AHEAD, true, HEA_SITE_HIST != 0>(
-        c, d.nbor, occ5, cnt_all, rec, stream, cur, d.Q, d.D, d.max_rounds, McTrace{nullptr, nullptr, 0}, rs, hist,
-        d.nbmask);
+    const McTally t = batch_search<T, L>(c, d, occ5, cnt_all, rec, stream, cur, rs, hist);
     unstage_occupancy(c, occ5, gocc);  // in place when hbm
     if (warp == 0)
         for (int x = lane; x < NC; x += 32) gcnt[x] = cnt_all[x];
