@@ -614,10 +614,9 @@ struct McResume {
 // copies in cnt_all).  Every thread returns the same f2/rounds/accepts; evals
 // is this thread's count.  No barrier at entry; one per round.  occ5 may be
 // shared or global memory; every thread writes the accepted swap's bytes
-// itself, so its own later loads see them either way.  kHist with kDrawHist:
-// the draws read the species from the histograms' species words (for an
-// occupancy in HBM), else from occ5.
-template <int T, class L, bool kAhead = false, bool kYield = false, bool kHist = false, bool kDrawHist = false>
+// itself, so its own later loads see them either way.  The draws read the
+// species from occ5.
+template <int T, class L, bool kAhead = false, bool kYield = false, bool kHist = false>
 __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *__restrict__ nbor, uint8_t *occ5,
                                              int32_t *cnt_all, SwapRecord *rec, uint32_t stream, double cur,
                                              int tasks, int depth, int64_t max_rounds, McTrace tr,
@@ -645,21 +644,14 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
         for (int q0 = warp * 32; q0 < tasks; q0 += blockDim.x) {
             const int q = q0 + lane;
             uint32_t s1 = 0, s2 = 0;
-            uint4 hp = make_uint4(0u, 0u, 0u, 0u), hq = hp;
-            const bool ok = q < tasks && ((kHist && kDrawHist)
-                                              ? draw_pair_hist(c, stream, (uint32_t)round, (uint32_t)q, hist, s1, s2, hp, hq)
-                                              : draw_pair(c, stream, (uint32_t)round, (uint32_t)q, occ5, s1, s2));
+            const bool ok = q < tasks && draw_pair(c, stream, (uint32_t)round, (uint32_t)q, occ5, s1, s2);
             __syncwarp();  // lanes that needed more draws rejoin before scoring
             double f = inf_d();
             uint32_t h1[S], h2[S];
             int m[S], a = 0, b = 0;
             if (ok) {
                 ++evals;
-                if constexpr (kHist && kDrawHist) {
-                    a = (int)hp.w / 5;
-                    b = (int)hq.w / 5;
-                    f = score_swap_hist<T, L>(c, nbor, hp, hq, nbmask, cnt, s1, s2, a, b, h1, h2, m);
-                } else if constexpr (kHist) {
+                if constexpr (kHist) {
                     a = occ5[s1] / 5;
                     b = occ5[s2] / 5;
                     f = score_swap_hist<T, L>(c, nbor, __ldcg(hist + s1), __ldcg(hist + s2), nbmask, cnt, s1, s2, a, b,
@@ -721,7 +713,7 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
                 cnt[x] += ((i == a) - (i == b)) * uj + ((j == a) - (j == b)) * ui;
             }
             if constexpr (kHist) {
-                update_hist<L, kDrawHist>(c, nbor, hist, w.s1, w.s2, a, b);
+                update_hist<L, false>(c, nbor, hist, w.s1, w.s2, a, b);
                 __syncthreads();  // next round's proposals read the updated counts and histograms
             } else {
                 __syncwarp();
