@@ -929,8 +929,11 @@ int plan_search(hea_plan *pl, hea_stats *stats)
 // the tasks are split over warps and passes), so the choice is a pure speed
 // question: each candidate (the default one task per thread, and 256 and 128
 // threads when smaller) searches a fresh generation-0 population for
-// kTuneRounds rounds; the highest evaluations per millisecond wins.  Picks
-// are cached per device and shape for the life of the process.
+// kTuneRounds rounds, once to warm up and kTunePasses times timed; a
+// candidate's rate is its best pass (evaluations per millisecond).  A smaller
+// CTA replaces the default only when its rate is above the default's by more
+// than kTuneMargin, so timing noise cannot trade the default for a near tie.
+// Picks are cached per device and shape for the life of the process.
 struct TuneKey {
     int dev, N, T, S, row4, Q, P;
     bool operator<(const TuneKey &o) const
@@ -940,7 +943,9 @@ struct TuneKey {
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, int> g_tune;
-constexpr int kTuneRounds = 48;
+constexpr int kTuneRounds = 200;
+constexpr int kTunePasses = 3;
+constexpr double kTuneMargin = 1.05;
 
 // With measure = false only a cached pick is applied (plans created without
 // HEA_FLAG_AUTOTUNE still use the pick of an earlier tuned plan of their shape).
@@ -969,10 +974,11 @@ int plan_autotune(hea_plan *pl, bool measure)
         const int64_t cap = saved.max_rounds > 0 ? std::min<int64_t>(saved.max_rounds, kTuneRounds) : kTuneRounds;
         pl->prm.max_rounds = cap;
         pl->prm.flags &= ~HEA_FLAG_TIME_KERNELS;
-        double best_rate = -1.0;
+        std::vector<double> rate_of(cand.size(), 0.0);
         int rc = HEA_OK;
-        for (int pass = 0; pass < 2 && rc == HEA_OK; ++pass) {  // pass 0 warms up
-            for (int b : cand) {
+        for (int pass = 0; pass <= kTunePasses && rc == HEA_OK; ++pass) {  // pass 0 warms up
+            for (size_t ci = 0; ci < cand.size(); ++ci) {
+                const int b = cand[ci];
                 pl->mc_block = b;
                 cudaMemsetAsync(pl->stats, 0, 4 * sizeof(unsigned long long), pl->stream);
                 iota_kernel<<<(2 * pl->P + 255) / 256, 256, 0, pl->stream>>>(pl->order, 2 * pl->P);
@@ -990,14 +996,17 @@ int plan_autotune(hea_plan *pl, bool measure)
                     break;
                 }
                 const double rate = ms > 0 ? st[1] / (double)ms : 0.0;
-                if (pass == 1 && rate > best_rate) {
-                    best_rate = rate;
-                    best = b;
-                }
+                if (pass > 0) rate_of[ci] = std::max(rate_of[ci], rate);
             }
         }
         pl->prm = saved;
         if (rc != HEA_OK) return rc;
+        double best_rate = rate_of[0] * kTuneMargin;  // cand[0] is the default
+        for (size_t ci = 1; ci < cand.size(); ++ci)
+            if (rate_of[ci] > best_rate) {
+                best_rate = rate_of[ci];
+                best = cand[ci];
+            }
     }
     pl->mc_block = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
