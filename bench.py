@@ -502,24 +502,28 @@ def main():
     h2d = (hp.nbor.nbytes + hp.shell_sizes.nbytes + hp.species.nbytes + hp.weight.nbytes + hp.target_sro.nbytes)
     d2h = out_occ.nbytes + out_fit.nbytes
 
-    # time to tolerance: the same search through the serving loop with fitness tolerance 1e-3
-    # (local searches and the request end once it is reached), submission to result on the host
+    # time to tolerance: the same search through the serving loop with a fitness tolerance (local
+    # searches and the request end once it is reached), submission to result on the host; 1e-3 is
+    # PyHEA's default threshold, the looser ones show the time along the way
     time_to_tol = None
+    time_to_tol_sweep = []
     if rank == 0:
         srv = hb.Server(max_requests=4, slice_ms=50.0)
         q = dict(num_solutions=st.P, total_iter=st.I, parallel_task=st.Q, converge_depth=st.D,
                  seed=replicas.replica_seed(rank, 20_000))
-        t0 = time.perf_counter()
-        rid = srv.submit(problem, q, tolerance=1e-3)
-        res = None
-        while res is None:
-            srv.step()
-            res = srv.result(rid)
-        tt = time.perf_counter() - t0
+        for tol in (1e-3, 1.02e-3, 1.1e-3, 1.5e-3):
+            t0 = time.perf_counter()
+            rid = srv.submit(problem, q, tolerance=tol)
+            res = None
+            while res is None:
+                srv.step()
+                res = srv.result(rid)
+            tt = time.perf_counter() - t0
+            time_to_tol_sweep.append({"tolerance": tol, "wall_ms": 1000.0 * tt, "iterations": res[2]["iterations"],
+                                      "best_fitness": float(res[1][0]), "reached": bool(res[1][0] <= tol),
+                                      "evals": res[2]["evals"]})
         srv.close()
-        time_to_tol = {"tolerance": 1e-3, "wall_ms": 1000.0 * tt, "iterations": res[2]["iterations"],
-                       "best_fitness": float(res[1][0]), "reached": bool(res[1][0] <= 1e-3),
-                       "evals": res[2]["evals"]}
+        time_to_tol = time_to_tol_sweep[0]
 
     dev = torch.device("cuda", local)
     total_ms_max, evals_all = replicas.combine(total_ms, evals, device=dev)
@@ -548,7 +552,7 @@ def main():
                          "kernel_share": mc_ms / total_ms if total_ms else None},
             "search": {"evals_per_step": evals / args.steps, "accepts_per_step": accepts / args.steps,
                        "best_fitness_last_step": float(best[0])},
-            "time_to_tol": time_to_tol,
+            "time_to_tol": time_to_tol, "time_to_tol_sweep": time_to_tol_sweep,
             "clocks": clocks,
         }
         # kernels launched per search: 1 generate + per iteration (generate, search, merge, search, sort), plus
