@@ -238,7 +238,7 @@ struct JobEnd {
 // One job of a structure with species count T and layout L.  Shared memory:
 // [occ5 (occ_stride + 16), unless hbm] | per-warp counts | swap records.
 #ifndef HEA_BATCH_AHEAD
-#define HEA_BATCH_AHEAD true  // whole-row loads before use (the batch kernel has 128 registers per thread)
+#define HEA_BATCH_AHEAD true  // gather form (HEA_SITE_HIST 0) only: whole-row loads before use
 #endif
 // The rounds of a job's local search in a call of their own: values the job
 // needs only before and after the search stay out of the loop's registers.

@@ -11,7 +11,7 @@ namespace hea {
 constexpr int kMaxTypes = 6;        // packed 5-bit histogram fields: 6 * 5 = 30 bits
 constexpr int kMaxShells = 3;       // pyhea builds three shells (pyhea/lattice/lattice.py:471-475)
 constexpr int kMaxShellPad = 28;    // padded shell length must stay below 32 (5-bit fields)
-constexpr uint32_t kPhiloxCallsPerDraw = 1u << 19;  // two attempts per call
+constexpr uint32_t kPhiloxCallsPerDraw = 1u << 19;  // two attempts per call (four with 16-bit draws)
 constexpr int kFeistelRounds = 6;
 constexpr uint32_t kInitStream = 0xFFFFFFFFu;
 
