@@ -37,10 +37,12 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes (read + write) per swap evaluation of mc_kernel on the plain GPU workload, from one
-# ncu capture (profiles/mc_kernel_bcc20_t5.md: 164.5 MB over a launch of 203.7 M evaluations);
-# reported per launch as roofline.traffic, scaled by the evaluations of the bench's launches.
-DRAM_BYTES_PER_EVAL = {"plain_gpu": 164.5e6 / 203.7e6}
+# DRAM bytes (read + write) per swap evaluation of the dominant kernel, from one ncu capture each,
+# reported per launch as roofline.traffic, scaled by the evaluations of the bench's launches:
+# mc_kernel on the plain GPU workload (profiles/mc_kernel_bcc20_t5.md: 164.5 MB over a launch of
+# 203.7 M evaluations); batch_kernel on the 64-structure batch, one iteration
+# (profiles/batch_kernel_batched64_dram.md: 152.5 GB over 631.3 M evaluations).
+DRAM_BYTES_PER_EVAL = {"plain_gpu": 164.5e6 / 203.7e6, "batched": 152.467e9 / 631.335e6}
 
 
 def parse_args():
@@ -242,6 +244,7 @@ def run_batched(args):
         b_ms += s["gpu_ms"]
         b_ev += s["evals"]
     clocks = sampler.stop()
+    evals_of = [0] * len(structs)  # per structure: the same proposals in both paths, so the same counts
     for k in range(args.steps):
         for i, plan in enumerate(plans):
             flush.zero_()
@@ -249,6 +252,7 @@ def run_batched(args):
             s = plan.run(seeds(args.warmup + k)[i])
             p_ms += s["gpu_ms"]
             p_ev += s["evals"]
+            evals_of[i] += s["evals"]
     # same seeds, same results: the last step of each path
     same = 0
     for i, plan in enumerate(plans):
@@ -258,6 +262,30 @@ def run_batched(args):
     batch.close()
     value = b_ev / (b_ms / 1000.0)
     plain = p_ev / (p_ms / 1000.0)
+
+    # end to end through the public API: every step creates the batch from the host problems
+    # (tables uploaded), runs it and reads every structure's population back to the host
+    e2e_s, e2e_ev = 0.0, 0
+    h2d = sum(pb.nbor.nbytes + pb.shell_sizes.nbytes + pb.species.nbytes + pb.weight.nbytes + pb.target_sro.nbytes
+              for pb in problems)
+    d2h = sum(st.P * (st.num_sites + 8) for st in structs)
+    for k in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eb = hb.Batch(problems, params)
+        s = eb.run(seeds(args.warmup + k))
+        for i in range(len(structs)):
+            eb.read(i)
+        eb.close()
+        e2e_s += time.perf_counter() - t0
+        e2e_ev += s["evals"]
+
+    # roofline of the persistent kernel: each structure's algorithmic bytes per evaluation
+    # (BCC 8/6/12 262 B, FCC 12/6/24 422 B) weighted by its evaluations, over the batch's device time
+    peak, peak_kind = measured_peaks()
+    alg_bytes = sum(e * st.evals_bytes() for e, st in zip(evals_of, structs)) / max(1, sum(evals_of)) * b_ev
+    achieved = alg_bytes / (b_ms / 1000.0) / 1e9
     line = {"metric": "swap_evals_per_sec", "value": value, "unit": "swap-evals/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": b_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -267,6 +295,12 @@ def run_batched(args):
             "plain": {"value": plain, "ms_per_step": p_ms / args.steps, "evals_per_step": p_ev / args.steps},
             "speedup_vs_plain": value / plain, "identical_structures": same, "structures": len(structs),
             "evals_per_step": b_ev / args.steps, "clocks": clocks,
+            "e2e": {"value": e2e_ev / e2e_s, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "kernel": "batch_kernel (persistent job engine)",
+                         "bytes_per_eval": alg_bytes / max(1, b_ev), "peak_kind": peak_kind,
+                         "traffic": DRAM_BYTES_PER_EVAL["batched"] * b_ev / args.steps},
             # one CUDA graph per step: queue reset, phase-0 seeding, the persistent kernel
             "gpu_launches": 3 * args.steps}
     print(json.dumps(line))
