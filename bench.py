@@ -263,17 +263,20 @@ def run_batched(args):
     value = b_ev / (b_ms / 1000.0)
     plain = p_ev / (p_ms / 1000.0)
 
-    # end to end through the public API: every step creates the batch from the host problems
-    # (tables uploaded), runs it and reads every structure's population back to the host
+    # end to end through the public API: every step creates the batch from the host problems in
+    # pinned memory (tables uploaded), runs it and reads every structure's population back
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    pinned = [hb.Problem(pin(pb.nbor), pin(pb.shell_sizes), pin(pb.species), pin(pb.weight), pin(pb.target_sro))
+              for pb in problems]
     e2e_s, e2e_ev = 0.0, 0
     h2d = sum(pb.nbor.nbytes + pb.shell_sizes.nbytes + pb.species.nbytes + pb.weight.nbytes + pb.target_sro.nbytes
-              for pb in problems)
+              for pb in pinned)
     d2h = sum(st.P * (st.num_sites + 8) for st in structs)
     for k in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        eb = hb.Batch(problems, params)
+        eb = hb.Batch(pinned, params)
         s = eb.run(seeds(args.warmup + k))
         for i in range(len(structs)):
             eb.read(i)
@@ -333,6 +336,26 @@ def run_large(args):
     clocks = sampler.stop()
     _, fit = plan.read()
     plan.close()
+
+    # end to end through the C ABI with pinned host buffers: the neighbour table uploaded and the
+    # population read back every step (same seeds as the device-timed steps, so the same work)
+    import numpy as np
+
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    hp = hb.Problem(pin(pb.nbor), pin(pb.shell_sizes), pin(pb.species), pin(pb.weight), pin(pb.target_sro))
+    out_occ = torch.empty((st.P, st.num_sites), dtype=torch.uint8).pin_memory().numpy()
+    out_fit = torch.empty(st.P, dtype=torch.float64).pin_memory().numpy()
+    e2e_s, e2e_ev = 0.0, 0
+    for k in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, _, s = hb.search(hp, st.P, 1, st.Q, st.D, seed=args.warmup + k, max_rounds=args.large_rounds,
+                            out_occ=out_occ, out_fitness=out_fit)
+        e2e_s += time.perf_counter() - t0
+        e2e_ev += s["evals"]
+    h2d = hp.nbor.nbytes + hp.shell_sizes.nbytes + hp.species.nbytes + hp.weight.nbytes + hp.target_sro.nbytes
+    d2h = out_occ.nbytes + out_fit.nbytes
+
     peak, peak_kind = measured_peaks()
     B = st.evals_bytes()
     achieved = ev * B / (mc_ms / 1000.0) / 1e9
@@ -347,6 +370,8 @@ def run_large(args):
                          "kernel": "mc_large_kernel (cluster local search)", "bytes_per_eval": B,
                          "peak_kind": peak_kind},
             "best_fitness_last_step": float(fit[0]), "evals_per_step": ev / args.steps, "clocks": clocks,
+            "e2e": {"value": e2e_ev / e2e_s, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
             # per step (one iteration): the slot-order reset; zero counts, generate, recount and fitness
             # for each of the two generations; two cluster local searches; merge and survivor sorts
             "gpu_launches": args.steps * 13}
