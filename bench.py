@@ -424,6 +424,8 @@ def run_serving(args):
     i, t0 = 0, time.perf_counter()
     hard_stop = args.serve_seconds + 120.0
     last_done = 0.0
+    lat_by_size = []  # (sites, latency ms)
+    step_gap, step_ms, t_prev = 0.0, 0.0, None  # longest gap between steps; longest step (host view)
     while True:
         now = time.perf_counter() - t0
         while i < len(reqs) and reqs[i][0] <= now:
@@ -439,7 +441,12 @@ def run_serving(args):
         if not arrival:
             time.sleep(max(0.0, min(reqs[i][0] - now, 0.002)))
             continue
+        ts = time.perf_counter()
+        if t_prev is not None:
+            step_gap = max(step_gap, ts - t_prev)
         srv.step()
+        t_prev = time.perf_counter()
+        step_ms = max(step_ms, (t_prev - ts) * 1000.0)
         for rid in srv.take_finished():
             if rid not in arrival:
                 continue
@@ -448,6 +455,7 @@ def run_serving(args):
             t = time.perf_counter() - t0
             lat.append((t - arrival.pop(rid)) * 1000.0)
             n, B = size.pop(rid)
+            lat_by_size.append((n, lat[-1]))
             evals += info["evals"]
             bytes_alg += info["evals"] * B
             iters.append(info["iterations"])
@@ -459,6 +467,14 @@ def run_serving(args):
     srv.close()
     wall = last_done
     lat_a = np.array(lat) if lat else np.array([float("nan")])
+
+    def pct(sel):  # p50 / p99 / max of the requests whose site count passes sel
+        v = np.array([ms for n, ms in lat_by_size if sel(n)])
+        if v.size == 0:
+            return None
+        return {"count": int(v.size), "p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)),
+                "max": float(v.max())}
+
     peak, peak_kind = measured_peaks()
     achieved = bytes_alg / (busy / 1000.0) / 1e9 if busy > 0 else 0.0
     value = evals / wall if wall > 0 else 0.0
@@ -474,7 +490,10 @@ def run_serving(args):
                          "per_s": len(lat) / wall if wall > 0 else 0.0,
                          "latency_ms": {"p50": float(np.percentile(lat_a, 50)), "p90": float(np.percentile(lat_a, 90)),
                                         "p99": float(np.percentile(lat_a, 99)), "max": float(lat_a.max())},
-                         "reached_tolerance_before_last_iteration": int(sum(1 for k in iters if k < I))},
+                         "reached_tolerance_before_last_iteration": int(sum(1 for k in iters if k < I)),
+                         "latency_ms_by_sites": {"below_1e5": pct(lambda n: n < 1e5),
+                                                 "from_1e5": pct(lambda n: n >= 1e5)},
+                         "host_longest_step_ms": step_ms, "host_longest_gap_between_steps_ms": step_gap * 1000.0},
             "gpu_busy_fraction": busy / (wall * 1000.0) if wall > 0 else 0.0,
             "e2e": {"value": value, "unit": "swap-evals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "note": "the serving line is end to end: one step = the whole run"},
