@@ -96,6 +96,33 @@ def test_full_search_bit_exact(case):
     assert stats["rounds"] == wstats["rounds"]
 
 
+@pytest.mark.parametrize("lat,cell,species", [
+    (L.BCC, 15, (2250, 2250, 2250)),     # 6750 sites: 2^16 mod N = 4786 > 4096
+    (L.BCC, 33, (23958, 23958, 23958)),  # 71 874 sites, above 2^16
+])
+def test_32bit_draws_bit_exact(lat, cell, species):
+    """Structures outside the 16-bit draw mode (two attempts per Philox call
+    from 32-bit words): trajectories and a whole search equal the oracle's."""
+    lib = ho.lib()
+    lib.hea_oracle_use_draw16.restype = ctypes.c_int
+    assert lib.hea_oracle_use_draw16(L.num_sites(lat, cell)) == 0
+    gp, op = pair((lat, cell, species, 3, L.SHELLS_REFERENCE), seed=1)
+    count, depth, call, tasks = 2, 4, 3, 64
+    occ0 = np.stack([op.generate(41, 1, s) for s in range(count)])
+    got = hb.local_search(gp, 41, call, occ0, tasks, depth, trace_cap=4096)
+    for s in range(count):
+        want = op.mc(41, (call << 16) | s, occ0[s], tasks, depth, trace_cap=4096)
+        assert got["rounds"][s] == want["rounds"] and got["trace"][s] == want["trace"]
+        np.testing.assert_array_equal(got["occ"][s], want["occ"])
+        np.testing.assert_array_equal(got["counts"][s], want["counts"])
+        assert got["f2"][s] == want["f2"]
+    occ, fit, stats = hb.search(gp, num_solutions=2, total_iter=1, parallel_task=48, converge_depth=3, seed=13)
+    wocc, wf2, wstats = op.hcs(13, 2, 1, 48, 3)
+    np.testing.assert_array_equal(occ, wocc)
+    np.testing.assert_array_equal(fit, np.sqrt(wf2))
+    assert stats["evals"] == wstats["evals"] and stats["rounds"] == wstats["rounds"]
+
+
 def test_plan_reruns_match_search():
     gp, _ = pair(CASES[0])
     occ, fit, _ = hb.search(gp, 6, 2, 48, 3, seed=5)
