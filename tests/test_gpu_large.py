@@ -17,6 +17,7 @@ pytestmark = pytest.mark.gpu
     (L.BCC, 6, (100, 100, 132, 100), 3, L.SHELLS_REFERENCE, 700),  # clusters of 2
     (L.FCC, 5, (100, 150, 250), 2, L.SHELLS_REFERENCE, 3000),      # clusters of 6
     (L.BCC, 4, (40, 44, 44), 1, L.SHELLS_REFERENCE, 4096),         # clusters of 8
+    (L.BCC, 33, (23958, 23958, 23958), 3, L.SHELLS_REFERENCE, 600),  # 71 874 sites: 32-bit draws
 ])
 def test_hbm_path_equals_shared_path_and_oracle(lat, cell, species, shells, shell_set, tasks):
     st = W.small_case(lattice=lat, cell=cell, species=species, shells=shells, shell_set=shell_set, seed=2)
