@@ -37,11 +37,12 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes (read + write) per swap evaluation of the dominant kernel, from one ncu capture each,
-# reported per launch as roofline.traffic, scaled by the evaluations of the bench's launches:
-# mc_kernel on the plain GPU workload (profiles/mc_kernel_bcc20_t5.md: 164.5 MB over a launch of
-# 203.7 M evaluations); batch_kernel on the 64-structure batch, one iteration
-# (profiles/batch_kernel_batched64_dram.md: 152.5 GB over 631.3 M evaluations).
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per swap evaluation of the dominant
+# kernel, from one ncu capture each, reported per launch as roofline.traffic, scaled by the
+# evaluations of the bench's launches: mc_kernel on the plain GPU workload, 164.5 MB over its first
+# local-search launch of 203.7 M evaluations (python -m pyhea_b200.cases plain --iters 1);
+# batch_kernel on the 64-structure batch, 152.5 GB over a launch of 631.3 M evaluations
+# (python -m pyhea_b200.cases batch --count 64 --iters 1).
 DRAM_BYTES_PER_EVAL = {"plain_gpu": 164.5e6 / 203.7e6, "batched": 152.467e9 / 631.335e6}
 
 
