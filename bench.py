@@ -245,7 +245,7 @@ def run_batched(args):
         b_ms += s["gpu_ms"]
         b_ev += s["evals"]
     clocks = sampler.stop()
-    evals_of = [0] * len(structs)  # per structure: the same proposals in both paths, so the same counts
+    evals_of = [int(t[1]) for t in batch.tallies()]  # per structure, last step
     for k in range(args.steps):
         for i, plan in enumerate(plans):
             flush.zero_()
@@ -253,7 +253,6 @@ def run_batched(args):
             s = plan.run(seeds(args.warmup + k)[i])
             p_ms += s["gpu_ms"]
             p_ev += s["evals"]
-            evals_of[i] += s["evals"]
     # same seeds, same results: the last step of each path
     same = 0
     for i, plan in enumerate(plans):
@@ -286,7 +285,8 @@ def run_batched(args):
         e2e_ev += s["evals"]
 
     # roofline of the persistent kernel: each structure's algorithmic bytes per evaluation
-    # (BCC 8/6/12 262 B, FCC 12/6/24 422 B) weighted by its evaluations, over the batch's device time
+    # (BCC 8/6/12 262 B, FCC 12/6/24 422 B) weighted by its evaluations in the batch's last step, over
+    # the batch's device time
     peak, peak_kind = measured_peaks()
     alg_bytes = sum(e * st.evals_bytes() for e, st in zip(evals_of, structs)) / max(1, sum(evals_of)) * b_ev
     achieved = alg_bytes / (b_ms / 1000.0) / 1e9

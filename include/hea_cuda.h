@@ -129,6 +129,10 @@ int hea_batch_run(hea_batch *batch, const uint64_t *seeds, hea_stats *stats);
 int hea_batch_read(hea_batch *batch, int32_t index, uint8_t *out_occ, double *out_fitness);
 /* Milliseconds from the start of the last run to each structure's final sort (device clock). */
 int hea_batch_finish_times(hea_batch *batch, double *out_ms);
+/* Per structure of the last run: local-search rounds, swap evaluations and
+ * accepted swaps, out[count][3] (the same counts as hea_stats of searching the
+ * structure alone with the same seed). */
+int hea_batch_tallies(hea_batch *batch, uint64_t *out);
 /* Autotuner of the batch's launch: times full runs (with the current seeds) for
  * occupancy kept in HBM or staged in shared memory where it fits, at the
  * kernel's resident CTAs per SM or one fewer, and keeps the fastest.  Results

@@ -114,6 +114,7 @@ def _declare(lib):
         "hea_batch_run": (_i32, [ctypes.c_void_p, _P(_u64), _P(Stats)]),
         "hea_batch_read": (_i32, [ctypes.c_void_p, _i32, _P(_u8), _P(_f64)]),
         "hea_batch_finish_times": (_i32, [ctypes.c_void_p, _P(_f64)]),
+        "hea_batch_tallies": (_i32, [ctypes.c_void_p, _P(_u64)]),
         "hea_batch_autotune": (_i32, [ctypes.c_void_p, _P(_i32), _P(_i32)]),
         "hea_batch_destroy": (None, [ctypes.c_void_p]),
         "hea_server_create": (_i32, [_P(_ServerConfig), _P(ctypes.c_void_p)]),
@@ -278,6 +279,12 @@ class Batch:
         """Milliseconds from the start of the last run to each structure's end."""
         out = np.empty(len(self.problems))
         _check(lib.hea_batch_finish_times(self._h, _ptr(out, _f64)))
+        return out
+
+    def tallies(self):
+        """Per structure of the last run: [rounds, swap evaluations, accepted swaps] (uint64 [count][3])."""
+        out = np.empty((len(self.problems), 3), dtype=np.uint64)
+        _check(lib.hea_batch_tallies(self._h, _ptr(out, _u64)))
         return out
 
     def close(self):

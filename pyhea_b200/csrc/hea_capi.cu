@@ -1793,6 +1793,16 @@ int hea_batch_finish_times(hea_batch *b, double *out_ms)
     return HEA_OK;
 }
 
+int hea_batch_tallies(hea_batch *b, uint64_t *out)
+{
+    if (!b || !out) return fail(HEA_ERR_INVALID, "batch and out must not be NULL");
+    std::vector<BatchState> st(b->count);
+    HEA_CUDA(cudaMemcpy(st.data(), b->d_states, sizeof(BatchState) * b->count, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < b->count; ++i)
+        for (int k = 0; k < 3; ++k) out[3 * i + k] = st[i].tally[k];
+    return HEA_OK;
+}
+
 void hea_batch_destroy(hea_batch *b) { delete b; }
 
 }  // extern "C"

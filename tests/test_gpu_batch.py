@@ -37,6 +37,7 @@ def test_batch_equals_plain_per_structure():
     seeds = [1000 + 17 * i for i in range(len(items))]
     b = hb.Batch([p for p, _ in items], [q for _, q in items])
     st = b.run(seeds)
+    tallies = b.tallies()
     total_evals = 0
     for i, (pb, q) in enumerate(items):
         occ, fit = b.read(i)
@@ -44,6 +45,7 @@ def test_batch_equals_plain_per_structure():
                                     seed=seeds[i])
         np.testing.assert_array_equal(occ, pocc, err_msg=f"structure {i}")
         np.testing.assert_array_equal(fit, pfit, err_msg=f"structure {i}")
+        assert list(tallies[i]) == [pst["rounds"], pst["evals"], pst["accepts"]], f"structure {i}"
         total_evals += pst["evals"]
     assert st["evals"] == total_evals
     # a second run with other seeds, then the first seeds again: same as before
