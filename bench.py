@@ -156,7 +156,7 @@ def cpu_reference_sample(st, nbor, sizes, procs, nnet_per_proc=5, step=1):
         pool.close()
     r["procs"] = procs
     r["sample"] = (f"{procs} processes x {nnet_per_proc} solutions x {step} iteration(s) of the same structure, "
-                   f"task={st.Q}, depth={st.D}; evaluations from rand() calls x (1 - sum c^2)")
+                   f"task={st.Q}, depth={st.D}; evaluations counted exactly (calls of the engine's incremental fitness)")
     return r
 
 
@@ -197,7 +197,7 @@ def run_reference(args):
     st = structs[0]
     what = "one structure of the mixed batch per step (cycling)" if args.workload == "batched" else "the full structure"
     sample = (f"per step: {procs} single-rank processes x {nnet} solutions x 1 iteration of {what}, "
-              f"task={st.Q}, depth={st.D}; evaluations = rand() calls / 2 x (1 - sum c^2)")
+              f"task={st.Q}, depth={st.D}; evaluations counted exactly (calls of the engine's incremental fitness)")
     line = {"metric": "swap_evals_per_sec", "value": value, "unit": "swap-evals/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * total_s / args.steps, "higher_is_better": True, "scaling": "weak",

@@ -237,18 +237,23 @@ int hea_local_search(const hea_problem *problem, uint64_t seed, uint32_t mc_call
                      int64_t *trace_len);
 
 /*
- * Allocation-free form of hea_recount (same arguments, same results).  It has
- * no counterpart in the reference.  It is for callers that cannot allocate
- * device memory -- a process whose GPU memory is reserved up front by another
- * allocator, or code that must not trigger cudaMalloc's device-wide
- * synchronisation -- and it never calls cudaMalloc or cudaFree: all its device
- * buffers live in one static device array of HEA_NOALLOC_SCRATCH_BYTES, which
- * every GPU that loads the library holds until the process exits.  The first
- * call on a device looks up that array's address (once per device, with the
- * device current); make it before any stream capture.  Inputs whose raw and
- * padded neighbour tables plus `count` occupancy rows, counts and f2 exceed
- * the array are rejected with HEA_ERR_UNSUPPORTED.  All calls share the array:
- * calls that overlap on the GPU (from two host threads) race.
+ * Allocation-free form of hea_recount (same arguments, same results; NULL
+ * out_counts or out_f2 are skipped, as there).  It has no counterpart in the
+ * reference.  It is for callers that cannot allocate device memory -- a
+ * process whose GPU memory is reserved up front by another allocator, or code
+ * that must not trigger cudaMalloc's device-wide synchronisation -- and it
+ * never calls cudaMalloc or cudaFree: all its device buffers live in one
+ * static device array of HEA_NOALLOC_SCRATCH_BYTES, which every GPU that
+ * loads the library holds until the process exits.  Every call looks up that
+ * array's address in the context current on the calling thread (so a device
+ * reset or another current context on the device is safe); the first call in
+ * a context loads the library's device code there, so make it before any
+ * stream capture.  Inputs whose raw and padded neighbour tables plus `count`
+ * occupancy rows, counts and f2 exceed the array are rejected with
+ * HEA_ERR_UNSUPPORTED.  All calls share the array and find the previous
+ * call's contents there (the error flag is cleared and the counts rebuilt
+ * from zero every call): calls that overlap on the GPU (from two host
+ * threads) race.
  */
 #define HEA_NOALLOC_SCRATCH_BYTES (16u << 20)
 int hea_recount_noalloc(const hea_problem *problem, int32_t count, const uint8_t *occ, int32_t *out_counts,

@@ -6,8 +6,9 @@ Produces
                                    reference's own pyhea/cpp/accelerate.cpp with
                                    ref_harness.cpp and the single-rank MPI stub
 
-The reference tree is read in place from REFERENCE_ROOT (default
-/root/reference); its sources are never copied.  When the tree is absent (as on
+The reference tree is read in place from REFERENCE_ROOT: the environment
+variable HEA_REFERENCE_ROOT, else a checkout named `reference` beside this
+repository; its sources are never copied.  When the tree is absent (as on
 a machine that only runs the prebuilt files) the reference library is left as
 it is.
 """
@@ -16,7 +17,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE_ROOT = os.environ.get("HEA_REFERENCE_ROOT", "/root/reference")
+REFERENCE_ROOT = os.environ.get("HEA_REFERENCE_ROOT") or os.path.join(os.path.dirname(os.path.dirname(HERE)),
+                                                                      "reference")
 
 
 def _run(cmd):

@@ -14,6 +14,7 @@
  *   accelerate::cpu::calculate_fitness_incremental accelerate.cpp:498-570
  *   accelerate::cpu::calculate_fitness_of_solutions accelerate.cpp:118-180
  *   accelerate::cpu::run_local_parallel_hcs        accelerate.cpp:713-763
+ * and counts the engine's swap evaluations (below).
  */
 #include <dlfcn.h>
 
@@ -37,6 +38,41 @@ extern "C" int rand(void) noexcept
     ++g_rand_calls;
     return real_rand();
 }
+
+/*
+ * Evaluation counter.  The reference's local search scores every proposal
+ * with one call of calculate_fitness_incremental (accelerate.cpp:659-661,
+ * an unqualified call on std::vector arguments).  Argument-dependent lookup
+ * at that call also finds the non-template function below, declared in the
+ * arguments' namespace before the reference source is read; with identical
+ * parameter types a non-template is preferred over the template, so each call
+ * passes through here, is counted, and runs the reference's own template.
+ */
+static unsigned long long g_fitness_calls = 0;
+namespace accelerate {
+namespace cpu {
+template <typename Integer, typename Real>
+Real calculate_fitness_incremental(std::vector<Integer> &lattice, std::vector<std::vector<std::vector<Real>>> &gamma,
+                                   const Integer &atom1, const Integer &atom2, const Integer &num_atoms,
+                                   const Integer &num_types, const Integer &num_shells,
+                                   const std::vector<Integer> &species,
+                                   const std::vector<std::vector<std::vector<Integer>>> &neighbor_list,
+                                   const std::vector<std::vector<Real>> &target_sro, const std::vector<Real> &weight);
+}  // namespace cpu
+}  // namespace accelerate
+namespace std {
+double calculate_fitness_incremental(vector<int> &lattice, vector<vector<vector<double>>> &gamma, const int &atom1,
+                                     const int &atom2, const int &num_atoms, const int &num_types,
+                                     const int &num_shells, const vector<int> &species,
+                                     const vector<vector<vector<int>>> &neighbor_list,
+                                     const vector<vector<double>> &target_sro, const vector<double> &weight)
+{
+    ++g_fitness_calls;
+    return accelerate::cpu::calculate_fitness_incremental<int, double>(lattice, gamma, atom1, atom2, num_atoms,
+                                                                       num_types, num_shells, species, neighbor_list,
+                                                                       target_sro, weight);
+}
+}  // namespace std
 
 #include "accelerate.cpp"
 
@@ -74,6 +110,9 @@ extern "C" {
 
 unsigned long long ref_rand_calls(void) { return g_rand_calls; }
 void ref_reset_rand_calls(void) { g_rand_calls = 0; }
+/* Swap evaluations (calls of the reference's incremental fitness) since the last reset. */
+unsigned long long ref_eval_count(void) { return g_fitness_calls; }
+void ref_reset_eval_count(void) { g_fitness_calls = 0; }
 
 /* gamma[i][j][k] (reference layout) of one occupancy. */
 int ref_recount(int num_sites, int num_types, int num_shells, const int32_t *nbor, int row,

@@ -1,12 +1,11 @@
 """Timing of the reference CPU engine (oracle/_ref/libref_accelerate.so).
 
 TEST INFRASTRUCTURE ONLY: used by bench.py for its CPU baseline and for the
-reference arm.  The reference engine has no swap-evaluation counter; it draws
-two rand() values per attempt and redraws both until the species differ
-(pyhea/cpp/accelerate.cpp:649-655), so an attempt succeeds with probability
-p = 1 - sum_t c_t^2 whatever the state (the composition never changes).  The
-evaluation count is estimated as rand_calls / 2 * p; its relative standard
-error is about sqrt((1 - p) / (p * evals)), below 1e-3 for any sample here.
+reference arm.  Swap evaluations are counted exactly: the harness counts the
+engine's calls of its incremental fitness, one per scored proposal
+(pyhea/cpp/accelerate.cpp:659-661).  The rand() call count is kept beside it as
+a cross-check: the engine draws two values per attempt and redraws until the
+species differ (:649-655), so evaluations ~ rand_calls / 2 * (1 - sum_t c_t^2).
 
 Multi-core follows the reference's own MPI split (accelerate.cpp:728): K
 independent single-rank processes, each searching its share of the
@@ -34,6 +33,7 @@ def _worker(job):
     os.dup2(devnull, 1)
     lib = ctypes.CDLL(REF_LIB)
     lib.ref_rand_calls.restype = ctypes.c_ulonglong
+    lib.ref_eval_count.restype = ctypes.c_ulonglong
     P = ctypes.POINTER
     i32 = lambda a: a.ctypes.data_as(P(ctypes.c_int32))  # noqa: E731
     f64 = lambda a: a.ctypes.data_as(P(ctypes.c_double))  # noqa: E731
@@ -41,12 +41,13 @@ def _worker(job):
     occ = np.zeros((nnet, n), dtype=np.int32)
     fit = np.zeros(nnet)
     lib.ref_reset_rand_calls()
+    lib.ref_reset_eval_count()
     t0 = time.perf_counter()
     lib.ref_run_local_parallel_hcs(nnet, step, task, depth, ctypes.c_double(0.001), n, len(species), len(weight),
                                    i32(nbor), nbor.shape[1], i32(shell_size), i32(species), f64(weight), f64(target),
                                    i32(occ), f64(fit))
     wall = time.perf_counter() - t0
-    return wall, int(lib.ref_rand_calls()), float(fit[0])
+    return wall, int(lib.ref_rand_calls()), float(fit[0]), int(lib.ref_eval_count())
 
 
 class RefPool:
@@ -70,7 +71,8 @@ class RefPool:
         c = species / species.sum()
         p_valid = 1.0 - float(np.sum(c * c))
         return {"wall_s": max(max(r[0] for r in res), 1e-9), "pool_wall_s": wall, "rand_calls": calls,
-                "evals": calls / 2.0 * p_valid, "best_fitness": min(r[2] for r in res)}
+                "evals": sum(r[3] for r in res), "evals_from_rand_calls": calls / 2.0 * p_valid,
+                "best_fitness": min(r[2] for r in res)}
 
     def close(self):
         self.pool.close()

@@ -9,8 +9,11 @@ Two front ends over one CUDA library (libhea_cuda.so, C ABI in include/hea_cuda.
   (``search``, ``Plan``, ``generate``, ``recount``, ``local_search``,
   ``build_neighbors``), used by the tests and the benchmark.
 
-Importing the package loads the CUDA library and raises ImportError when it has
-not been built (``python pyhea_b200/build.py``); there is no CPU fallback.
+The CUDA library is loaded on first use -- any call below, or the ``lib`` and
+``accelerate`` attributes -- and raises ImportError then when it has not been
+built (``python pyhea_b200/build.py``); there is no CPU fallback.  Importing the
+package, or its numpy-only modules (``lattice``, ``workloads``, ``sro``,
+``output``), maps no shared library.
 """
 import ctypes
 import os
@@ -19,8 +22,6 @@ import numpy as np
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_PKG, "libhea_cuda.so")
-if not os.path.exists(_LIB_PATH):
-    raise ImportError(f"{_LIB_PATH} is missing; build it with `python pyhea_b200/build.py`")
 
 _P = ctypes.POINTER
 _i32, _i64, _u32, _u64, _f64, _u8 = (ctypes.c_int32, ctypes.c_int64, ctypes.c_uint32, ctypes.c_uint64,
@@ -135,18 +136,38 @@ def _declare(lib):
     return lib
 
 
-lib = _declare(ctypes.CDLL(_LIB_PATH))
-from . import accelerate  # noqa: E402  (pybind11 module next to the library)
+_lib = None
+
+
+def _load():
+    """The CUDA library with its C ABI declared; loaded on the first call."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise ImportError(f"{_LIB_PATH} is missing; build it with `python pyhea_b200/build.py`")
+        _lib = _declare(ctypes.CDLL(_LIB_PATH))
+    return _lib
+
+
+def __getattr__(name):
+    if name == "lib":
+        return _load()
+    if name == "accelerate":  # pybind11 module next to the library; it links the library itself
+        import importlib
+
+        _load()
+        return importlib.import_module(".accelerate", __name__)
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")
 
 
 def _check(rc):
     if rc != HEA_OK:
-        msg = lib.hea_last_error().decode()
+        msg = _load().hea_last_error().decode()
         raise (HeaValueError if rc == HEA_ERR_INVALID else HeaError)(rc, msg)
 
 
 def cuda_available():
-    return bool(lib.hea_cuda_available())
+    return bool(_load().hea_cuda_available())
 
 
 def _ptr(a, ct):
@@ -193,7 +214,7 @@ def search(problem, num_solutions, total_iter, parallel_task, converge_depth, se
     flags = ((HEA_FLAG_LOG_ITERS if log else 0) | (HEA_FLAG_TIME_KERNELS if time_kernels else 0) |
              (HEA_FLAG_HBM_OCCUPANCY if hbm_occupancy else 0))
     prm = _params(P, total_iter, parallel_task, converge_depth, seed, max_rounds, flags)
-    _check(lib.hea_run_local_parallel_hcs(ctypes.byref(problem._c), ctypes.byref(prm), _ptr(occ, _u8),
+    _check(_load().hea_run_local_parallel_hcs(ctypes.byref(problem._c), ctypes.byref(prm), _ptr(occ, _u8),
                                           _ptr(fit, _f64), ctypes.byref(st)))
     return occ, fit, st.as_dict()
 
@@ -209,27 +230,27 @@ class Plan:
         flags = ((HEA_FLAG_TIME_KERNELS if time_kernels else 0) | (HEA_FLAG_HBM_OCCUPANCY if hbm_occupancy else 0)
                  | (HEA_FLAG_AUTOTUNE if autotune else 0))
         prm = _params(num_solutions, total_iter, parallel_task, converge_depth, seed, max_rounds, flags)
-        _check(lib.hea_plan_create(ctypes.byref(problem._c), ctypes.byref(prm), ctypes.byref(self._h)))
+        _check(_load().hea_plan_create(ctypes.byref(problem._c), ctypes.byref(prm), ctypes.byref(self._h)))
 
     @property
     def local_search_block(self):
         """Threads per CTA of the local search (the autotuner's pick when autotune=True)."""
-        return int(lib.hea_plan_local_search_block(self._h))
+        return int(_load().hea_plan_local_search_block(self._h))
 
     def run(self, seed):
         st = Stats()
-        _check(lib.hea_plan_run(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, ctypes.byref(st)))
+        _check(_load().hea_plan_run(self._h, int(seed) & 0xFFFFFFFFFFFFFFFF, ctypes.byref(st)))
         return st.as_dict()
 
     def read(self):
         occ = np.empty((self.P, self.problem.num_sites), dtype=np.uint8)
         fit = np.empty(self.P, dtype=np.float64)
-        _check(lib.hea_plan_read(self._h, _ptr(occ, _u8), _ptr(fit, _f64)))
+        _check(_load().hea_plan_read(self._h, _ptr(occ, _u8), _ptr(fit, _f64)))
         return occ, fit
 
     def close(self):
         if self._h:
-            lib.hea_plan_destroy(self._h)
+            _load().hea_plan_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):
@@ -254,42 +275,42 @@ class Batch:
                                             q["converge_depth"], 0, q.get("max_rounds", 0)) for q in params])
         self.P = [int(q["num_solutions"]) for q in params]
         self._h = ctypes.c_void_p()
-        _check(lib.hea_batch_create(self._pb, self._prm, n, ctypes.byref(self._h)))
+        _check(_load().hea_batch_create(self._pb, self._prm, n, ctypes.byref(self._h)))
 
     def run(self, seeds):
         arr = (_u64 * len(self.problems))(*[int(s) & 0xFFFFFFFFFFFFFFFF for s in seeds])
         st = Stats()
-        _check(lib.hea_batch_run(self._h, arr, ctypes.byref(st)))
+        _check(_load().hea_batch_run(self._h, arr, ctypes.byref(st)))
         return st.as_dict()
 
     def read(self, index):
         occ = np.empty((self.P[index], self.problems[index].num_sites), dtype=np.uint8)
         fit = np.empty(self.P[index], dtype=np.float64)
-        _check(lib.hea_batch_read(self._h, int(index), _ptr(occ, _u8), _ptr(fit, _f64)))
+        _check(_load().hea_batch_read(self._h, int(index), _ptr(occ, _u8), _ptr(fit, _f64)))
         return occ, fit
 
     def autotune(self):
         """Time the launch configurations on full runs (current seeds) and keep the fastest;
         returns {"hbm_all": 0|1, "ctas_per_sm": n}.  Results do not depend on it."""
         h, c = _i32(), _i32()
-        _check(lib.hea_batch_autotune(self._h, ctypes.byref(h), ctypes.byref(c)))
+        _check(_load().hea_batch_autotune(self._h, ctypes.byref(h), ctypes.byref(c)))
         return {"hbm_all": h.value, "ctas_per_sm": c.value}
 
     def finish_times(self):
         """Milliseconds from the start of the last run to each structure's end."""
         out = np.empty(len(self.problems))
-        _check(lib.hea_batch_finish_times(self._h, _ptr(out, _f64)))
+        _check(_load().hea_batch_finish_times(self._h, _ptr(out, _f64)))
         return out
 
     def tallies(self):
         """Per structure of the last run: [rounds, swap evaluations, accepted swaps] (uint64 [count][3])."""
         out = np.empty((len(self.problems), 3), dtype=np.uint64)
-        _check(lib.hea_batch_tallies(self._h, _ptr(out, _u64)))
+        _check(_load().hea_batch_tallies(self._h, _ptr(out, _u64)))
         return out
 
     def close(self):
         if self._h:
-            lib.hea_batch_destroy(self._h)
+            _load().hea_batch_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):
@@ -314,7 +335,7 @@ class Server:
         cfg = _ServerConfig(int(max_requests), int(ring_jobs), int(arena_bytes), int(smem_bytes), int(hbm_sites),
                             float(slice_ms))
         self._h = ctypes.c_void_p()
-        _check(lib.hea_server_create(ctypes.byref(cfg), ctypes.byref(self._h)))
+        _check(_load().hea_server_create(ctypes.byref(cfg), ctypes.byref(self._h)))
         self._meta = {}  # id -> (P, N)
 
     @staticmethod
@@ -325,7 +346,7 @@ class Server:
     def submit(self, problem, params, tolerance=-1.0, priority=0):
         prm = self._prm(params)
         rid = _i64()
-        _check(lib.hea_server_submit(self._h, ctypes.byref(problem._c), ctypes.byref(prm), float(tolerance),
+        _check(_load().hea_server_submit(self._h, ctypes.byref(problem._c), ctypes.byref(prm), float(tolerance),
                                      int(priority), ctypes.byref(rid)))
         self._meta[rid.value] = (int(params["num_solutions"]), problem.num_sites)
         return rid.value
@@ -340,7 +361,7 @@ class Server:
             raise ValueError(f"target_sro needs {S}*{T}*{T} values, got {tg.size}")
         prm = self._prm(params)
         rid = _i64()
-        _check(lib.hea_server_submit_lattice(self._h, int(lattice), int(cell), int(shell_set), T, S, _ptr(sp, _i32),
+        _check(_load().hea_server_submit_lattice(self._h, int(lattice), int(cell), int(shell_set), T, S, _ptr(sp, _i32),
                                              _ptr(w, _f64), _ptr(tg, _f64), ctypes.byref(prm), float(tolerance),
                                              int(priority), ctypes.byref(rid)))
         n = (4 if lattice == FCC else 2) * int(cell) ** 3
@@ -351,19 +372,19 @@ class Server:
         """Wait for the previous time slice, hand over its finished requests, admit queued ones and
         launch the next slice (not waited for); returns the number of requests that finished."""
         fin = _i32()
-        _check(lib.hea_server_step(self._h, ctypes.byref(fin)))
+        _check(_load().hea_server_step(self._h, ctypes.byref(fin)))
         return fin.value
 
     def take_finished(self, cap=4096):
         """Ids of requests that finished (or failed) since the last call."""
         ids = (_i64 * cap)()
         n = _i32()
-        _check(lib.hea_server_take_finished(self._h, ids, int(cap), ctypes.byref(n)))
+        _check(_load().hea_server_take_finished(self._h, ids, int(cap), ctypes.byref(n)))
         return list(ids[: n.value])
 
     def info(self, rid):
         inf = RequestInfo()
-        _check(lib.hea_server_info(self._h, int(rid), ctypes.byref(inf)))
+        _check(_load().hea_server_info(self._h, int(rid), ctypes.byref(inf)))
         return inf.as_dict()
 
     def result(self, rid):
@@ -372,7 +393,7 @@ class Server:
         occ = np.empty((P, n), dtype=np.uint8)
         fit = np.empty(P, dtype=np.float64)
         inf = RequestInfo()
-        rc = lib.hea_server_result(self._h, int(rid), _ptr(occ, _u8), _ptr(fit, _f64), ctypes.byref(inf))
+        rc = _load().hea_server_result(self._h, int(rid), _ptr(occ, _u8), _ptr(fit, _f64), ctypes.byref(inf))
         if rc == HEA_PENDING:
             return None
         self._meta.pop(rid, None)
@@ -381,7 +402,7 @@ class Server:
 
     def status(self):
         st = ServerStatus()
-        _check(lib.hea_server_status_get(self._h, ctypes.byref(st)))
+        _check(_load().hea_server_status_get(self._h, ctypes.byref(st)))
         return st.as_dict()
 
     def drain(self, max_steps=1 << 30):
@@ -395,7 +416,7 @@ class Server:
 
     def close(self):
         if self._h:
-            lib.hea_server_destroy(self._h)
+            _load().hea_server_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):
@@ -410,25 +431,34 @@ def generate(problem, seed, generation, count):
     occ = np.empty((count, problem.num_sites), dtype=np.uint8)
     cnt = np.empty((count, problem.num_shells, problem.num_types, problem.num_types), dtype=np.int32)
     f2 = np.empty(count)
-    _check(lib.hea_generate(ctypes.byref(problem._c), int(seed), int(generation), int(count), _ptr(occ, _u8),
+    _check(_load().hea_generate(ctypes.byref(problem._c), int(seed), int(generation), int(count), _ptr(occ, _u8),
                             _ptr(cnt, _i32), _ptr(f2, _f64)))
     return occ, cnt, f2
 
 
+def _rows(problem, occ):
+    """Occupancies as a contiguous uint8 [count][N] array; N must be the problem's site count
+    (the C ABI reads exactly count x N bytes)."""
+    occ = np.ascontiguousarray(np.atleast_2d(occ), dtype=np.uint8)
+    if occ.ndim != 2 or occ.shape[1] != problem.num_sites:
+        raise ValueError(f"occupancies must be [count][{problem.num_sites}], got shape {occ.shape}")
+    return occ
+
+
 def recount(problem, occ):
     """hea_recount: (counts [count][S][T][T], f2 [count]) of occupancies [count][N]."""
-    occ = np.ascontiguousarray(np.atleast_2d(occ), dtype=np.uint8)
+    occ = _rows(problem, occ)
     count = occ.shape[0]
     cnt = np.empty((count, problem.num_shells, problem.num_types, problem.num_types), dtype=np.int32)
     f2 = np.empty(count)
-    _check(lib.hea_recount(ctypes.byref(problem._c), int(count), _ptr(occ, _u8), _ptr(cnt, _i32), _ptr(f2, _f64)))
+    _check(_load().hea_recount(ctypes.byref(problem._c), int(count), _ptr(occ, _u8), _ptr(cnt, _i32), _ptr(f2, _f64)))
     return cnt, f2
 
 
 def local_search(problem, seed, mc_call, occ, tasks, depth, max_rounds=0, trace_cap=0, trace_counts=False):
     """hea_local_search on occupancies [count][N] (copied).  Returns a dict with
     occ, counts, f2, rounds and, when trace_cap > 0, per-occupancy traces."""
-    occ = np.array(np.atleast_2d(occ), dtype=np.uint8, copy=True)
+    occ = np.array(_rows(problem, occ), copy=True)
     count = occ.shape[0]
     cnt = np.empty((count, problem.num_shells, problem.num_types, problem.num_types), dtype=np.int32)
     f2 = np.empty(count)
@@ -437,7 +467,7 @@ def local_search(problem, seed, mc_call, occ, tasks, depth, max_rounds=0, trace_
     tc = (np.empty((count, trace_cap, problem.num_shells, problem.num_types, problem.num_types), dtype=np.int32)
           if trace_cap and trace_counts else None)
     tlen = np.zeros(count, dtype=np.int64) if trace_cap else None
-    _check(lib.hea_local_search(ctypes.byref(problem._c), int(seed), int(mc_call), int(count), int(tasks), int(depth),
+    _check(_load().hea_local_search(ctypes.byref(problem._c), int(seed), int(mc_call), int(count), int(tasks), int(depth),
                                 int(max_rounds), _ptr(occ, _u8), _ptr(cnt, _i32), _ptr(f2, _f64), _ptr(rounds, _i64),
                                 tr, _ptr(tc, _i32), int(trace_cap), _ptr(tlen, _i64)))
     out = {"occ": occ, "counts": cnt, "f2": f2, "rounds": rounds}
@@ -457,11 +487,11 @@ def recount_noalloc(problem, occ):
     """hea_recount_noalloc: the same results as recount() from a fixed static
     device array instead of allocated buffers (for callers that cannot
     allocate device memory)."""
-    occ = np.ascontiguousarray(np.atleast_2d(occ), dtype=np.uint8)
+    occ = _rows(problem, occ)
     count = occ.shape[0]
     cnt = np.empty((count, problem.num_shells, problem.num_types, problem.num_types), dtype=np.int32)
     f2 = np.empty(count)
-    _check(lib.hea_recount_noalloc(ctypes.byref(problem._c), int(count), _ptr(occ, _u8), _ptr(cnt, _i32),
+    _check(_load().hea_recount_noalloc(ctypes.byref(problem._c), int(count), _ptr(occ, _u8), _ptr(cnt, _i32),
                                    _ptr(f2, _f64)))
     return cnt, f2
 
@@ -471,8 +501,8 @@ def build_neighbors(lattice, cell, shell_set=SHELLS_REFERENCE):
     (nbor int32 [N][sum Z], shell_sizes int32 [3])."""
     sizes = np.zeros(3, dtype=np.int32)
     n = _i32()
-    _check(lib.hea_build_neighbors(int(lattice), int(cell), int(shell_set), None, _ptr(sizes, _i32), ctypes.byref(n)))
+    _check(_load().hea_build_neighbors(int(lattice), int(cell), int(shell_set), None, _ptr(sizes, _i32), ctypes.byref(n)))
     nbor = np.empty((n.value, int(sizes.sum())), dtype=np.int32)
-    _check(lib.hea_build_neighbors(int(lattice), int(cell), int(shell_set), _ptr(nbor, _i32), _ptr(sizes, _i32),
+    _check(_load().hea_build_neighbors(int(lattice), int(cell), int(shell_set), _ptr(nbor, _i32), _ptr(sizes, _i32),
                                    ctypes.byref(n)))
     return nbor, sizes

@@ -1286,24 +1286,16 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[HEA_NOALLOC_SCR
 
 namespace {
 
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-void *g_noalloc_ptr[kNoAllocMaxDevices] = {};
-
-// Device address of the scratch array on the current device, looked up once
-// per device with that device current.
+// Device address of the scratch array in the context current on this thread,
+// looked up on every call: the address belongs to one context, so a cached one
+// would be stale after a device reset or under another current context (a
+// driver-API context on the same device), and the lookup costs far less than
+// the call's synchronous copies.
 int noalloc_scratch(void **out)
 {
-    int dev = 0;
-    HEA_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(HEA_ERR_UNSUPPORTED, "device %d out of range", dev);
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
-        void *p = nullptr;
-        HEA_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_noalloc_ptr[dev] = p;
-    }
-    *out = g_noalloc_ptr[dev];
+    void *p = nullptr;
+    HEA_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    *out = p;
     return HEA_OK;
 }
 
@@ -1315,7 +1307,7 @@ extern "C" int hea_recount_noalloc(const hea_problem *problem, int32_t count, co
                                    double *out_f2)
 {
     if (count < 1 || count > 65535) return fail(HEA_ERR_INVALID, "count must be 1..65535");
-    if (!occ || !out_counts || !out_f2) return fail(HEA_ERR_INVALID, "occ, out_counts and out_f2 must not be NULL");
+    if (!occ) return fail(HEA_ERR_INVALID, "occ is NULL");
     HEA_TRY(validate_problem(problem));
     const hea_problem *pb = problem;
     const int T = pb->num_types, S = pb->num_shells, N = pb->num_sites;
@@ -1428,8 +1420,11 @@ extern "C" int hea_recount_noalloc(const hea_problem *problem, int32_t count, co
     a.generate = 0;
     gen<<<count, 512, smem>>>(c, a);
     HEA_CUDA(cudaGetLastError());
-    HEA_CUDA(cudaMemcpy(out_counts, d_cnt, (size_t)count * ncount * sizeof(int32_t), cudaMemcpyDeviceToHost));
-    HEA_CUDA(cudaMemcpy(out_f2, d_f2, (size_t)count * sizeof(double), cudaMemcpyDeviceToHost));
+    // NULL outputs are skipped, as hea_recount skips them
+    if (out_counts)
+        HEA_CUDA(cudaMemcpy(out_counts, d_cnt, (size_t)count * ncount * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (out_f2) HEA_CUDA(cudaMemcpy(out_f2, d_f2, (size_t)count * sizeof(double), cudaMemcpyDeviceToHost));
+    HEA_CUDA(cudaDeviceSynchronize());
     return HEA_OK;
 }
 

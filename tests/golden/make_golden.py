@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a checkout that has the reference tree (default /root/reference, or
-HEA_REFERENCE_ROOT) and the reference CPU engine built by
+Run in a checkout that has the reference tree (HEA_REFERENCE_ROOT, else a
+checkout named `reference` beside this repository) and the reference CPU engine built by
 oracle/build_oracle.py:
 
     python oracle/build_oracle.py && python tests/golden/make_golden.py
@@ -38,7 +38,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE_ROOT = os.environ.get("HEA_REFERENCE_ROOT", "/root/reference")
+REFERENCE_ROOT = os.environ.get("HEA_REFERENCE_ROOT") or os.path.join(os.path.dirname(REPO), "reference")
 
 
 def import_reference():

@@ -72,6 +72,35 @@ def test_batch_matches_oracle_on_one_structure():
     b.close()
 
 
+def test_batch_matches_oracle_for_every_kernel_instance():
+    """One structure of every (species count, shell layout) the batch engine
+    compiles -- T = 2..6 on the BCC 8/6/12 and FCC 12/6/24 layouts of the mixed
+    batch and on the runtime layouts (FCC 12/6/12, two shells, one shell) --
+    in one batch, each equal to the oracle's whole search."""
+    specs = [(L.BCC, 4, L.SHELLS_REFERENCE, 3), (L.FCC, 3, L.SHELLS_FCC_TRUE3, 3), (L.FCC, 3, L.SHELLS_REFERENCE, 3),
+             (L.BCC, 4, L.SHELLS_REFERENCE, 2), (L.FCC, 3, L.SHELLS_REFERENCE, 1)]
+    rng = np.random.default_rng(11)
+    items = []
+    for lat, cell, shell_set, S in specs:
+        for T in range(2, 7):
+            n = L.num_sites(lat, cell)
+            st = W.small_case(lattice=lat, cell=cell, species=W.dirichlet_counts(rng, T, n), shells=S,
+                              shell_set=shell_set, seed=len(items))
+            nbor, sizes = st.neighbors()
+            q = dict(num_solutions=3, total_iter=2, parallel_task=int(rng.choice([24, 64, 130])), converge_depth=3)
+            items.append((hb.Problem(nbor, sizes, st.species, st.weight, st.target), q))
+    seeds = [300 + i for i in range(len(items))]
+    b = hb.Batch([p for p, _ in items], [q for _, q in items])
+    b.run(seeds)
+    for i, (pb, q) in enumerate(items):
+        occ, fit = b.read(i)
+        op = ho.Problem(pb.nbor, pb.shell_sizes, pb.species, pb.weight, pb.target_sro)
+        wocc, wf2, _ = op.hcs(seeds[i], q["num_solutions"], q["total_iter"], q["parallel_task"], q["converge_depth"])
+        np.testing.assert_array_equal(occ, wocc, err_msg=f"structure {i}")
+        np.testing.assert_array_equal(fit, np.sqrt(wf2), err_msg=f"structure {i}")
+    b.close()
+
+
 def test_autotuned_batch_gives_the_same_results():
     """The batch autotuner only changes where occupancies live and how many CTAs share an SM."""
     items = mixed_structures(4, 5)

@@ -27,7 +27,12 @@ CASES = [
     (L.BCC, 4, (40, 44, 44), 2, L.SHELLS_REFERENCE),
     (L.FCC, 4, (100, 156), 1, L.SHELLS_REFERENCE),
     (L.BCC, 3, (1, 53), 3, L.SHELLS_REFERENCE),  # 54 sites (not a multiple of 16), one minority atom
+    # the layouts and species counts of the benchmarked structures: BCC 8/6/12 with 5 species
+    # (mc_kernel<5, Shells<2,2,3>>) and FCC 12/6/24 with 4 species (mc_kernel<4, Shells<3,2,6>>)
+    (L.BCC, 5, (50, 50, 50, 50, 50), 3, L.SHELLS_REFERENCE),
+    (L.FCC, 3, (27, 27, 27, 27), 3, L.SHELLS_FCC_TRUE3),
 ]
+FULL_SEARCH_CASES = CASES[:4] + CASES[6:]
 
 
 def pair(case, seed=0):
@@ -85,7 +90,7 @@ def test_local_search_trajectory_bit_exact(case, tasks):
         np.testing.assert_array_equal(got["counts"][s], op.recount(got["occ"][s]))
 
 
-@pytest.mark.parametrize("case", CASES[:4])
+@pytest.mark.parametrize("case", FULL_SEARCH_CASES)
 def test_full_search_bit_exact(case):
     gp, op = pair(case)
     occ, fit, stats = hb.search(gp, num_solutions=4, total_iter=2, parallel_task=32, converge_depth=4, seed=77)
