@@ -34,10 +34,18 @@
  *   Fitness    f2 = sum_k w_k * sum_i sum_j d^2 with d = fma(-C', R, E),
  *              E = 1 - target, R = N / (Z_k * n_i * n_j), accumulated with
  *              fma per shell over the upper triangle row by row (d_ii, then
- *              d_ij, d_ji for j > i).  Fitness reported = sqrt(f2); every
- *              comparison is made on f2.
- *   Ties       lowest task index wins the round (strict <), accept iff strictly
- *              better; populations are sorted stably by f2.
+ *              d_ij, d_ji for j > i).  Fitness reported = sqrt(f2).
+ *   Scoring    a proposal is scored by D, the change of f2 its swap makes,
+ *              from the rank-2 form of the count change (hea_oracle_delta
+ *              below): the same quantity as the reference's full fitness of
+ *              the swapped counts (accelerate.cpp:555-569) minus the current
+ *              one, in O(T) terms per shell, with a fixed operation order.
+ *   Ties       the round's best proposal is the lowest D, lowest task index
+ *              on ties; it is accepted iff D < 0 (the reference accepts iff
+ *              the new fitness is strictly below the current one,
+ *              accelerate.cpp:678); the search's running f2 adds D, and the
+ *              f2 stored at its end is recomputed from the counts.
+ *              Populations are sorted stably by f2.
  */
 #include <math.h>
 #include <stdint.h>
@@ -318,6 +326,148 @@ void hea_oracle_swap_counts(const hea_oracle_problem *p, const uint8_t *occ, uin
 }
 
 /* ------------------------------------------------------------------------ */
+/* Swap delta                                                                 */
+/* ------------------------------------------------------------------------ */
+/*
+ * Swapping species a (site s1) and b (site s2) changes the counts of shell k
+ * only in rows and columns a and b: dC_ij = sa_i u_j + sa_j u_i with
+ * sa = e_a - e_b, so that u_t = dC_at for t != a, b, u_a = dC_aa / 2 and
+ * u_b = -dC_bb / 2.  Expanding sum_ij (d_ij - R_ij dC_ij)^2 - d_ij^2 with
+ * d = E - R C and R symmetric gives, per shell,
+ *     sum_t u_t (L_t + u_t Q_t) + (u_a - u_b)^2 Cq
+ * with L_t = -2 (G_at - G_bt), G_it = R_it (d_it + d_ti),
+ * Q_t = 2 (R_at^2 + R_bt^2) (t != a, b), Q_a = 4 R_aa^2, Q_b = 4 R_bb^2,
+ * Cq = 2 R_ab^2; the weights w_k multiply L, Q and Cq.  The tables below hold
+ * them for every shell and ordered pair (a, b); L is rebuilt from the counts
+ * after every accepted swap.  Operation order (shared with the kernels):
+ *     Q = w * (2 * (R_at*R_at + R_bt*R_bt)),  Q_a = w * (4 * (R_aa*R_aa)),
+ *     Cq = w * (2 * (R_ab*R_ab)),
+ *     d_it = fma(-C_it, R_it, E_it), d_ti = fma(-C_it, R_it, E_ti),
+ *     G_it = R_it * (d_it + d_ti),  L = (-2 * w) * (G_at - G_bt),
+ *     D = 0; per shell, per t: D = fma(u_t, fma(u_t, Q_t, L_t), D);
+ *     then D = fma((u_a - u_b)^2, Cq, D).
+ */
+typedef struct {
+    int T, S;
+    double *L;  /* [S][T][T][T]  (k, a, b, t) */
+    double *Q;  /* [S][T][T][T] */
+    double *Cq; /* [S][T][T] */
+} delta_tables;
+
+static int delta_alloc(const hea_oracle_problem *p, delta_tables *d)
+{
+    size_t n3 = (size_t)p->num_shells * p->num_types * p->num_types * p->num_types;
+    d->T = p->num_types;
+    d->S = p->num_shells;
+    d->L = (double *)calloc(n3, sizeof(double));
+    d->Q = (double *)calloc(n3, sizeof(double));
+    d->Cq = (double *)calloc((size_t)p->num_shells * p->num_types * p->num_types, sizeof(double));
+    return d->L && d->Q && d->Cq;
+}
+
+static void delta_free(delta_tables *d)
+{
+    free(d->L);
+    free(d->Q);
+    free(d->Cq);
+}
+
+static void delta_constants(const hea_oracle_problem *p, delta_tables *d)
+{
+    int T = d->T;
+    for (int k = 0; k < d->S; ++k) {
+        const double *R = p->R + (size_t)k * T * T;
+        double w = p->weight[k];
+        for (int a = 0; a < T; ++a)
+            for (int b = 0; b < T; ++b) {
+                if (a == b) continue;
+                size_t row = ((size_t)(k * T + a) * T + b);
+                d->Cq[row] = w * (2.0 * (R[a * T + b] * R[a * T + b]));
+                for (int t = 0; t < T; ++t) {
+                    double q;
+                    if (t == a || t == b)
+                        q = w * (4.0 * (R[t * T + t] * R[t * T + t]));
+                    else
+                        q = w * (2.0 * (R[a * T + t] * R[a * T + t] + R[b * T + t] * R[b * T + t]));
+                    d->Q[row * T + t] = q;
+                }
+            }
+    }
+}
+
+static void delta_linear(const hea_oracle_problem *p, const int32_t *C, delta_tables *d)
+{
+    int T = d->T;
+    double *G = (double *)malloc(sizeof(double) * (size_t)T * T);
+    for (int k = 0; k < d->S; ++k) {
+        const double *R = p->R + (size_t)k * T * T, *E = p->E + (size_t)k * T * T;
+        const int32_t *Ck = C + (size_t)k * T * T;
+        for (int i = 0; i < T; ++i)
+            for (int t = 0; t < T; ++t) {
+                double c = (double)Ck[i * T + t];
+                double dit = fma(-c, R[i * T + t], E[i * T + t]);
+                double dti = fma(-c, R[i * T + t], E[t * T + i]);
+                G[i * T + t] = R[i * T + t] * (dit + dti);
+            }
+        double m2w = -2.0 * p->weight[k];
+        for (int a = 0; a < T; ++a)
+            for (int b = 0; b < T; ++b) {
+                if (a == b) continue;
+                for (int t = 0; t < T; ++t)
+                    d->L[((size_t)(k * T + a) * T + b) * T + t] = m2w * (G[a * T + t] - G[b * T + t]);
+            }
+    }
+    free(G);
+}
+
+/* D of the swap whose counts before and after are C and Cp (a at s1, b at s2). */
+static double delta_of(const delta_tables *d, const int32_t *C, const int32_t *Cp, int a, int b)
+{
+    int T = d->T;
+    double D = 0.0;
+    for (int k = 0; k < d->S; ++k) {
+        const int32_t *c0 = C + (size_t)k * T * T, *c1 = Cp + (size_t)k * T * T;
+        size_t row = (size_t)(k * T + a) * T + b;
+        int ua = 0, ub = 0;
+        for (int t = 0; t < T; ++t) {
+            int u;
+            if (t == a)
+                u = (c1[a * T + a] - c0[a * T + a]) / 2;
+            else if (t == b)
+                u = -(c1[b * T + b] - c0[b * T + b]) / 2;
+            else
+                u = c1[a * T + t] - c0[a * T + t];
+            if (t == a) ua = u;
+            if (t == b) ub = u;
+            double ud = (double)u;
+            D = fma(ud, fma(ud, d->Q[row * T + t], d->L[row * T + t]), D);
+        }
+        D = fma((double)((ua - ub) * (ua - ub)), d->Cq[row], D);
+    }
+    return D;
+}
+
+/*
+ * D of swapping s1 and s2 (species must differ) in the state (occ, C): the
+ * tables are built from C, the swapped counts by the reference's update.
+ */
+double hea_oracle_delta(const hea_oracle_problem *p, const uint8_t *occ, const int32_t *C, uint32_t s1, uint32_t s2)
+{
+    size_t ncount = (size_t)p->num_shells * p->num_types * p->num_types;
+    delta_tables d;
+    int32_t *cp = (int32_t *)malloc(sizeof(int32_t) * ncount);
+    if (!cp || !delta_alloc(p, &d)) return NAN;
+    delta_constants(p, &d);
+    delta_linear(p, C, &d);
+    memcpy(cp, C, sizeof(int32_t) * ncount);
+    hea_oracle_swap_counts(p, occ, s1, s2, cp);
+    double D = delta_of(&d, C, cp, occ[s1], occ[s2]);
+    delta_free(&d);
+    free(cp);
+    return D;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Local parallel Monte Carlo on one solution (accelerate.cpp:626-692)       */
 /* ------------------------------------------------------------------------ */
 typedef struct {
@@ -327,9 +477,11 @@ typedef struct {
 
 /*
  * Runs the swap search on one occupancy in place.  C holds its counts on entry
- * and on exit; *f2 its fitness.  Returns the number of rounds; each round scores
+ * and on exit; *f2 its fitness on entry and, on exit, the fitness recomputed
+ * from the final counts.  Returns the number of rounds; each round scores
  * `tasks` proposals.  When trace != NULL up to trace_cap accepted swaps are
- * written there (and, when trace_counts != NULL, the counts after each of them).
+ * written there with the running f2 after each (and, when trace_counts !=
+ * NULL, the counts after each of them).
  */
 int64_t hea_oracle_mc(const hea_oracle_problem *p, const uint32_t key[2], uint32_t stream, int tasks, int depth,
                       int64_t max_rounds, uint8_t *occ, int32_t *C, double *f2, hea_oracle_accept *trace,
@@ -338,11 +490,15 @@ int64_t hea_oracle_mc(const hea_oracle_problem *p, const uint32_t key[2], uint32
     size_t ncount = (size_t)p->num_shells * p->num_types * p->num_types;
     int32_t *cp = (int32_t *)malloc(sizeof(int32_t) * ncount);
     int32_t *cbest = (int32_t *)malloc(sizeof(int32_t) * ncount);
+    delta_tables d;
+    if (!cp || !cbest || !delta_alloc(p, &d)) return -1;
+    delta_constants(p, &d);
+    delta_linear(p, C, &d);
     double cur = *f2;
     int64_t rounds = 0, acc = 0, evals = 0;
     int miss = 0;
     while (miss < depth && rounds < max_rounds) {
-        double best = INFINITY;
+        double best = 0.0;
         int64_t bq = -1;
         uint32_t b1 = 0, b2 = 0;
         for (int q = 0; q < tasks; ++q) {
@@ -352,28 +508,29 @@ int64_t hea_oracle_mc(const hea_oracle_problem *p, const uint32_t key[2], uint32
             ++evals;
             memcpy(cp, C, sizeof(int32_t) * ncount);
             hea_oracle_swap_counts(p, occ, s1, s2, cp);
-            double f = hea_oracle_f2(p, cp);
-            if (f < best) {
-                best = f;
+            double D = delta_of(&d, C, cp, occ[s1], occ[s2]);
+            if (D < 0.0 && (bq < 0 || D < best)) {
+                best = D;
                 bq = q;
                 b1 = s1;
                 b2 = s2;
                 memcpy(cbest, cp, sizeof(int32_t) * ncount);
             }
         }
-        if (bq >= 0 && best < cur) {
+        if (bq >= 0) {
             uint8_t t = occ[b1];
             occ[b1] = occ[b2];
             occ[b2] = t;
             memcpy(C, cbest, sizeof(int32_t) * ncount);
-            cur = best;
+            delta_linear(p, C, &d);
+            cur = cur + best;
             miss = 0;
             if (trace && acc < trace_cap) {
                 trace[acc].round = (uint32_t)rounds;
                 trace[acc].task = (uint32_t)bq;
                 trace[acc].s1 = b1;
                 trace[acc].s2 = b2;
-                trace[acc].f2 = best;
+                trace[acc].f2 = cur;
                 if (trace_counts) memcpy(trace_counts + (size_t)acc * ncount, C, sizeof(int32_t) * ncount);
             }
             ++acc;
@@ -384,7 +541,8 @@ int64_t hea_oracle_mc(const hea_oracle_problem *p, const uint32_t key[2], uint32
     }
     free(cp);
     free(cbest);
-    *f2 = cur;
+    delta_free(&d);
+    *f2 = hea_oracle_f2(p, C);
     if (n_accepts) *n_accepts = acc;
     if (n_evals) *n_evals = evals;
     return rounds;

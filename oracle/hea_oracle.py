@@ -34,6 +34,7 @@ def _load():
 
     lib = ctypes.CDLL(build_oracle())
     lib.hea_oracle_f2.restype = f64
+    lib.hea_oracle_delta.restype = f64
     lib.hea_oracle_draw_pair.restype = i64
     lib.hea_oracle_mc.restype = i64
     lib.hea_oracle_permute.restype = u32
@@ -113,6 +114,12 @@ class Problem:
         lib().hea_oracle_swap_counts(ctypes.byref(self._c), _ptr(occ, u8), u32(s1), u32(s2), _ptr(Cp, i32))
         return Cp
 
+    def delta(self, occ, C, s1, s2):
+        """D: the change of f2 swapping s1 and s2 makes, by the scoring contract (rank-2 form)."""
+        occ = np.ascontiguousarray(occ, dtype=np.uint8)
+        C = np.ascontiguousarray(C, dtype=np.int32)
+        return lib().hea_oracle_delta(ctypes.byref(self._c), _ptr(occ, u8), _ptr(C, i32), u32(s1), u32(s2))
+
     def draw_pair(self, seed, stream, rnd, task, occ):
         occ = np.ascontiguousarray(occ, dtype=np.uint8)
         a, b = u32(), u32()
@@ -121,7 +128,8 @@ class Problem:
         return (int(att), a.value, b.value)
 
     def mc(self, seed, stream, occ, tasks, depth, max_rounds=1 << 30, trace_cap=0, trace_counts=False):
-        """Search one occupancy (copied); returns dict with occ, counts, f2, rounds, accepts, evals, trace."""
+        """Search one occupancy (copied); returns dict with occ, counts, f2 (recomputed from the final
+        counts), rounds, accepts, evals and the trace (round, task, s1, s2, running f2 after the swap)."""
         occ = np.array(occ, dtype=np.uint8, copy=True)
         C = self.recount(occ)
         f2 = f64(self.f2(C))

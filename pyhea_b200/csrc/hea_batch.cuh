@@ -236,20 +236,17 @@ struct JobEnd {
 };
 
 // One job of a structure with species count T and layout L.  Shared memory:
-// [occ5 (occ_stride + 16), unless hbm] | per-warp counts | swap records.
-#ifndef HEA_BATCH_AHEAD
-#define HEA_BATCH_AHEAD true  // gather form (HEA_SITE_HIST 0) only: whole-row loads before use
-#endif
+// [occ5 (occ_stride + 16), unless hbm] | search_smem_tail(T, S, nwarps) (delta
+// table, swap records, two count buffers).
 // The rounds of a job's local search in a call of their own: values the job
 // needs only before and after the search stay out of the loop's registers.
 template <int T, class L>
-__device__ __noinline__ McTally batch_search(const SearchConst &c, const BatchStruct &d, uint8_t *occ5,
-                                             int32_t *cnt_all, SwapRecord *rec, uint32_t stream, double cur,
+__device__ __noinline__ McTally batch_search(const SearchConst &c, const BatchStruct &d, uint8_t *occ5, int32_t *cnt2,
+                                             double2 *tab, SwapRecord *rec, uint32_t stream, double cur,
                                              const McResume rs, uint4 *hist)
 {
-    return mc_rounds<T, L, HEA_BATCH_AHEAD, true, HEA_SITE_HIST != 0>(
-        c, d.nbor, occ5, cnt_all, rec, stream, cur, d.Q, d.D, d.max_rounds, McTrace{nullptr, nullptr, 0}, rs, hist,
-        d.nbmask);
+    return mc_rounds<T, L, true>(c, d.nbor, occ5, cnt2, tab, rec, stream, cur, d.Q, d.D, d.max_rounds,
+                                 McTrace{nullptr, nullptr, 0}, rs, hist, d.nbmask);
 }
 
 template <int T, class L>
@@ -258,7 +255,7 @@ __device__ __noinline__ JobEnd batch_job(const SearchConst &c, const BatchStruct
                                          unsigned long long deadline)
 {
     constexpr int S = L::S, NC = S * T * T, NCP = mc_ncount_pad(NC);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int nwarps = blockDim.x >> 5;
     const bool hbm = d.hbm != 0;
     const int P = d.P, n = c.num_sites;
     const int pos = job.index;
@@ -267,47 +264,43 @@ __device__ __noinline__ JobEnd batch_job(const SearchConst &c, const BatchStruct
     int32_t *gcnt = d.cnt + (size_t)slot * NC;
     uint4 *hist = d.hist + (size_t)slot * c.num_sites;
     uint8_t *occ5 = hbm ? gocc : smem;
-    int32_t *cnt_all = reinterpret_cast<int32_t *>(hbm ? smem : smem + c.occ_stride + 16);
-    SwapRecord *rec = reinterpret_cast<SwapRecord *>(cnt_all + nwarps * NCP);
+    double2 *tab = reinterpret_cast<double2 *>(hbm ? smem : smem + c.occ_stride + 16);
+    SwapRecord *rec = reinterpret_cast<SwapRecord *>(tab + delta_entries(T, S));
+    int32_t *cnt2 = reinterpret_cast<int32_t *>(rec + 2 * nwarps);
 
     double cur;
     if (job.kind == kJobMc2 || job.resume) {
         stage_occupancy<true>(c, gocc, occ5);  // in place when hbm
-        for (int x = lane; x < NC; x += 32) cnt_all[warp * NCP + x] = __ldcg(gcnt + x);
+        for (int x = threadIdx.x; x < NC; x += blockDim.x) cnt2[x] = __ldcg(gcnt + x);
         __syncthreads();
         if (threadIdx.x == 0) occ5[n] = 0;  // sentinel
-        cur = __ldcg(d.f2 + slot);
-        __syncthreads();
+        cur = __ldcg(d.f2 + slot);  // a resumed search's running f2
     } else {
         const uint32_t generation = job.kind == kJobGen0 ? 0u : (uint32_t)(job.iter + 1);
         generate_occupancy<T>(c, (uint32_t)pos, generation, occ5, (job.kind == kJobGen0 && !hbm) ? gocc : nullptr);
         if (threadIdx.x == 0) occ5[n] = 0;
         __syncthreads();
-        block_recount<T, S>(c, d.nbor, occ5, cnt_all, hist);  // copy 0; ends with a barrier
-        cur = fitness_of_counts<T, S>(c, cnt_all);
+        block_recount<T, S>(c, d.nbor, occ5, cnt2, hist);  // count buffer 0; ends with a barrier
+        cur = fitness_of_counts<T, S>(c, cnt2);
         if (job.kind == kJobGen0) {
             if (hbm) unstage_occupancy(c, occ5, gocc);
-            if (warp == 0)
-                for (int x = lane; x < NC; x += 32) gcnt[x] = cnt_all[x];
+            for (int x = threadIdx.x; x < NC; x += blockDim.x) gcnt[x] = cnt2[x];
             if (threadIdx.x == 0) d.f2[slot] = cur;
             return JobEnd{0, 0, 0};
         }
-        for (int x = lane; x < NC; x += 32)
-            if (warp) cnt_all[warp * NCP + x] = cnt_all[x];
-        __syncthreads();
     }
+    search_setup<T, S>(c, cnt2, tab);
     const uint32_t call = job.kind == kJobMc2 ? (uint32_t)(2 * job.iter + 1) : (uint32_t)(2 * job.iter);
     const uint32_t stream = (call << 16) | (uint32_t)pos;
     const McResume rs{job.resume ? (int64_t)job.round0 : 0, job.resume ? job.miss0 : 0, deadline, d.tol2};
     // the draws read the species from the occupancy: measured on the mixed batch, the histograms'
     // species words (draw_pair_hist) were slower for every structure size
-    const McTally t = batch_search<T, L>(c, d, occ5, cnt_all, rec, stream, cur, rs, hist);
+    const McTally t = batch_search<T, L>(c, d, occ5, cnt2, tab, rec, stream, cur, rs, hist);
     unstage_occupancy(c, occ5, gocc);  // in place when hbm
-    if (warp == 0)
-        for (int x = lane; x < NC; x += 32) gcnt[x] = cnt_all[x];
+    for (int x = threadIdx.x; x < NC; x += blockDim.x) gcnt[x] = cnt2[t.buf * NCP + x];
     add_tally(t, stats);
     add_tally(t, tally);
-    if (threadIdx.x == 0) d.f2[slot] = t.f2;
+    if (threadIdx.x == 0) d.f2[slot] = t.f2;  // recomputed from the counts, or the running f2 of a yielded search
     return JobEnd{t.yielded ? 1 : 0, (int32_t)t.round_end, t.miss};
 }
 

@@ -504,9 +504,11 @@ int smem_limit()
     return v;
 }
 
-size_t mc_smem(int occ_stride, int ncount, int nwarps)
+// Dynamic shared memory of mc_kernel: occupancy + sentinel, then the search's
+// delta table, swap records and count buffers.
+size_t mc_smem(int occ_stride, int T, int S, int nwarps)
 {
-    return (size_t)occ_stride + 16 + (size_t)nwarps * (4 * mc_ncount_pad(ncount) + 2 * sizeof(SwapRecord));
+    return (size_t)occ_stride + 16 + search_smem_tail(T, S, nwarps);
 }
 
 int choose_block(int tasks)
@@ -593,7 +595,7 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t
     // shared memory of the two kernels
     const size_t cnt_bytes = 4 * (size_t)((dt.ncount + 3) & ~3);
     dt.smem_gen = (size_t)c.occ_stride + 16 + cnt_bytes;
-    dt.smem_mc = mc_smem(c.occ_stride, (int)dt.ncount, 16);  // the largest block (512 threads)
+    dt.smem_mc = mc_smem(c.occ_stride, T, S, 16);  // the largest block (512 threads)
     if (dt.smem_mc > (size_t)smem_limit() || (flags & HEA_FLAG_HBM_OCCUPANCY)) {
         // structures beyond shared memory: occupancy in HBM, cluster search
         dt.large = true;
@@ -747,8 +749,7 @@ int launch_mc(hea_plan *pl, const int32_t *order, int count, uint32_t mc_call, M
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(count * csize);
         cfg.blockDim = dim3(block);
-        cfg.dynamicSmemBytes = (size_t)nw * (4 * mc_ncount_pad((int)pl->dt.ncount) + 2 * sizeof(SwapRecord)) +
-                               2 * sizeof(SwapRecord);
+        cfg.dynamicSmemBytes = search_smem_tail(pl->dt.T, pl->dt.S, nw) + 2 * sizeof(SwapRecord);
         cfg.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -760,7 +761,7 @@ int launch_mc(hea_plan *pl, const int32_t *order, int count, uint32_t mc_call, M
         HEA_CUDA(cudaLaunchKernelEx(&cfg, pl->dt.mc, pl->dt.c, a));
     } else {
         const int block = pl->mc_block;
-        pl->dt.mc<<<count, block, mc_smem(pl->dt.c.occ_stride, (int)pl->dt.ncount, block / 32), st>>>(pl->dt.c, a);
+        pl->dt.mc<<<count, block, mc_smem(pl->dt.c.occ_stride, pl->dt.T, pl->dt.S, block / 32), st>>>(pl->dt.c, a);
     }
     HEA_CUDA(cudaGetLastError());
     if (timed) {
@@ -799,7 +800,7 @@ int plan_alloc(hea_plan *pl, int slots)
         dev_alloc(&pl->out_f2, (size_t)slots * sizeof(double)) != cudaSuccess ||
         dev_alloc(&pl->stats, 4 * sizeof(unsigned long long)) != cudaSuccess)
         return fail(HEA_ERR_NOMEM, "cannot allocate the population buffers (%zu bytes of occupancy)", occ_bytes);
-    if (HEA_SITE_HIST && dev_alloc(&pl->hist, (size_t)slots * c.num_sites * sizeof(uint4)) != cudaSuccess)
+    if (dev_alloc(&pl->hist, (size_t)slots * c.num_sites * sizeof(uint4)) != cudaSuccess)
         return fail(HEA_ERR_NOMEM, "cannot allocate the site histograms (%zu bytes)",
                     (size_t)slots * c.num_sites * sizeof(uint4));
     HEA_CUDA(cudaMemsetAsync(pl->occ, 0, occ_bytes, pl->stream));
@@ -1516,11 +1517,11 @@ int batch_layout(const SearchConst &c, int S)
     return S == 1 ? kLayRt1 : (S == 2 ? kLayRt2 : kLayRt3);
 }
 
-// Shared memory of one batch job: occupancy (unless it stays in HBM), per-warp
-// counts and the double-buffered swap records.
-size_t batch_job_smem(int occ_stride, int64_t ncount, int nwarps, bool hbm)
+// Shared memory of one batch job: occupancy (unless it stays in HBM), then the
+// search's delta table, swap records and count buffers.
+size_t batch_job_smem(int occ_stride, int T, int S, int nwarps, bool hbm)
 {
-    return (hbm ? 0 : (size_t)occ_stride + 16) + (size_t)nwarps * (4 * mc_ncount_pad((int)ncount) + 2 * sizeof(SwapRecord));
+    return (hbm ? 0 : (size_t)occ_stride + 16) + search_smem_tail(T, S, nwarps);
 }
 
 // Dynamic shared memory per CTA that still lets HEA_BATCH_MIN_BLOCKS batch CTAs
@@ -1552,9 +1553,9 @@ int batch_configure(hea_batch *b, int hbm_all, int ctas_per_sm)
     size_t smem = 0;
     for (int i = 0; i < b->count; ++i) {
         BatchStruct &d = b->h_structs[i];
-        const int64_t ncount = b->tables[i]->ncount;
-        d.hbm = (hbm_all || batch_job_smem(d.c.occ_stride, ncount, nwarps, false) > budget) ? 1 : 0;
-        smem = std::max(smem, batch_job_smem(d.c.occ_stride, ncount, nwarps, d.hbm != 0));
+        const int T = b->tables[i]->T, S = b->tables[i]->S;
+        d.hbm = (hbm_all || batch_job_smem(d.c.occ_stride, T, S, nwarps, false) > budget) ? 1 : 0;
+        smem = std::max(smem, batch_job_smem(d.c.occ_stride, T, S, nwarps, d.hbm != 0));
     }
     cudaFuncAttributes a;
     HEA_CUDA(cudaFuncGetAttributes(&a, batch_kernel));
@@ -1684,7 +1685,7 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
     // only for its draws, and small shared memory leaves room for more CTAs per
     // SM and a larger L1 (measured faster on the mixed batch; hea_batch_autotune
     // compares the alternatives on the batch at hand).
-    if (rc == HEA_OK) rc = batch_configure(b, HEA_SITE_HIST ? 1 : 0, HEA_BATCH_MIN_BLOCKS);
+    if (rc == HEA_OK) rc = batch_configure(b, 1, HEA_BATCH_MIN_BLOCKS);
     if (rc != HEA_OK) {
         delete b;
         return rc;
@@ -2099,7 +2100,7 @@ int server_place(hea_server *sv, ServerRequest &r, int slot)
     d.T = r.T;
     d.layout = batch_layout(c, r.S);
     d.level = r.level;
-    d.hbm = (batch_job_smem(c.occ_stride, (int64_t)r.S * r.T * r.T, sv->nwarps, false) > sv->smem ||
+    d.hbm = (batch_job_smem(c.occ_stride, r.T, r.S, sv->nwarps, false) > sv->smem ||
              sv->cfg.hbm_sites == 0 || (sv->cfg.hbm_sites > 0 && r.N >= sv->cfg.hbm_sites))
                 ? 1
                 : 0;
@@ -2331,7 +2332,7 @@ int hea_server_create(const hea_server_config *config, hea_server **out)
     size_t budget = 0;
     if (rc == HEA_OK) rc = batch_smem_budget(&budget);
     if (rc == HEA_OK) {
-        const size_t least = batch_job_smem(0, (int64_t)kMaxShells * kMaxTypes * kMaxTypes, sv->nwarps, true);
+        const size_t least = batch_job_smem(0, kMaxTypes, kMaxShells, sv->nwarps, true);
         sv->smem = cfg.smem_bytes > 0 ? (size_t)cfg.smem_bytes : (cfg.hbm_sites == 0 ? least : budget);
         sv->smem = std::max(sv->smem, least);
         cudaFuncAttributes a;

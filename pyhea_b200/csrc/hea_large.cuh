@@ -15,8 +15,8 @@
 //     row during the search are those swaps);
 //   * generation and recount are grid-wide over sites (many CTAs per solution);
 //     the recount also writes the site histograms the search scores from
-//     (hist, see score_swap_hist), which rank 0 of the cluster updates after
-//     every accepted swap, followed by a cluster barrier.
+//     (hist, see score_delta), which rank 0 of the cluster updates after every
+//     accepted swap, followed by a cluster barrier.
 #pragma once
 #include <cooperative_groups.h>
 
@@ -111,7 +111,10 @@ __global__ void large_fitness_kernel(const SearchConst c, const int32_t *order, 
 }
 
 // The local search with the occupancy in HBM, one cluster per solution.
-// Shared memory: nwarps * (4 * ncount_pad + 2 * sizeof(SwapRecord)) + 2 * sizeof(SwapRecord).
+// Shared memory: search_smem_tail(T, S, nwarps) + 2 * sizeof(SwapRecord):
+// delta table, the warps' records [2][nwarps], two count buffers, and this
+// CTA's best record [2] (read by the cluster).  Every CTA keeps its own copy of
+// the table and counts and applies each accepted swap to them itself.
 template <int T, class L>
 __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, const McArgs g)
 {
@@ -121,17 +124,15 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
     const int rank = (int)cluster.block_rank(), csize = (int)cluster.num_blocks();
     const int sol = blockIdx.x / csize;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    int32_t *cnt_all = reinterpret_cast<int32_t *>(smem);
-    // with site histograms an accept ends with a cluster barrier anyway, so one shared copy of the
-    // counts, updated by the whole CTA, replaces the per-warp copies
-    int32_t *cnt = HEA_SITE_HIST ? cnt_all : cnt_all + warp * NCP;
-    SwapRecord *rec = reinterpret_cast<SwapRecord *>(cnt_all + nwarps * NCP);  // [2][nwarps]
-    SwapRecord *cta_rec = rec + 2 * nwarps;                                      // [2]: this CTA's best
+    double2 *tab = reinterpret_cast<double2 *>(smem);
+    SwapRecord *rec = reinterpret_cast<SwapRecord *>(tab + delta_entries(T, S));  // [2][nwarps]
+    int32_t *cnt2 = reinterpret_cast<int32_t *>(rec + 2 * nwarps);                // [2][NCP]
+    SwapRecord *cta_rec = reinterpret_cast<SwapRecord *>(cnt2 + 2 * NCP);         // [2]: this CTA's best
 
     const int slot = g.order[sol];
     const uint32_t stream = (g.mc_call << 16) | (uint32_t)sol;
     uint8_t *row = g.occ + (size_t)slot * c.occ_stride;
-    uint4 *hist = g.hist ? g.hist + (size_t)slot * c.num_sites : nullptr;
+    uint4 *hist = g.hist + (size_t)slot * c.num_sites;
     int32_t *gcnt = g.cnt + (size_t)slot * NC;
     const int n = c.num_sites;
     // this CTA's share of the row and of the tasks
@@ -139,17 +140,19 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
     const int qpart = (g.tasks + csize - 1) / csize, qlo = rank * qpart, qhi = min(g.tasks, qlo + qpart);
 
     for (int s = lo + tid; s < hi; s += blockDim.x) row[s] = (uint8_t)(5 * row[s]);
-    for (int x = HEA_SITE_HIST ? tid : lane; x < NC; x += HEA_SITE_HIST ? blockDim.x : 32) cnt[x] = gcnt[x];
+    for (int x = tid; x < NC; x += blockDim.x) cnt2[x] = gcnt[x];
+    __syncthreads();
+    search_setup<T, S>(c, cnt2, tab);
     cluster.sync();
 
     double cur = g.f2[slot];
-    int miss = 0;
+    int miss = 0, buf = 0;
     int64_t round = 0, accepts = 0, evals = 0;
     while (miss < g.depth && round < g.max_rounds) {
         SwapRecord *rr = rec + (round & 1) * nwarps;
         SwapRecord &mine = rr[warp];
         if (lane == 0) {
-            mine.f2 = inf_d();
+            mine.key = kNoSwap;
             mine.task = 0x7FFFFFFF;
         }
         __syncwarp();
@@ -157,43 +160,34 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
             const int q = q0 + lane;
             uint32_t s1 = 0, s2 = 0;
             uint4 hp = make_uint4(0u, 0u, 0u, 0u), hq = hp;
-            // with histograms the species come from their species words: one L2 round trip per attempt
-            const bool ok = q < qhi && (HEA_SITE_HIST != 0
-                                            ? draw_pair_hist(c, stream, (uint32_t)round, (uint32_t)q, hist, s1, s2, hp, hq)
-                                            : draw_pair(c, stream, (uint32_t)round, (uint32_t)q, row, s1, s2));
+            // the species come from the histograms' species words: one L2 round trip per attempt
+            const bool ok = q < qhi && draw_pair_hist(c, stream, (uint32_t)round, (uint32_t)q, hist, s1, s2, hp, hq);
             __syncwarp();
-            double f = inf_d();
+            uint64_t key = kNoSwap;
             uint32_t h1[S], h2[S];
-            int m[S], a = 0, b = 0;
+            int a = 0, b = 0;
             if (ok) {
                 ++evals;
-                if constexpr (HEA_SITE_HIST != 0) {
-                    a = (int)hp.w / 5;
-                    b = (int)hq.w / 5;
-                    f = score_swap_hist<T, L>(c, g.nbor, hp, hq, g.nbmask, cnt, s1, s2, a, b, h1, h2, m);
-                } else {
-                    a = row[s1] / 5;
-                    b = row[s2] / 5;
-                    f = score_swap<T, L>(c, g.nbor, row, cnt, s1, s2, a, b, h1, h2, m);
-                }
+                a = (int)hp.w / 5;
+                b = (int)hq.w / 5;
+                key = delta_key(score_delta<T, L>(c, g.nbor, g.nbmask, tab, hp, hq, s1, s2, a, b, h1, h2));
             }
-            double wf = f;
-            int wq = ok ? q : 0x7FFFFFFF;
-            warp_argmin(wf, wq);
-            if (ok && wq == q && better(wf, wq, mine.f2, mine.task)) {
+            uint64_t wk = key;
+            int wq = key != kNoSwap ? q : 0x7FFFFFFF;
+            warp_argmin(wk, wq);
+            if (key != kNoSwap && wq == q && better(wk, wq, mine.key, mine.task)) {
                 SwapRecord r;
-                r.f2 = wf;
+                r.key = wk;
                 r.task = wq;
                 r.s1 = s1;
                 r.s2 = s2;
                 r.ab = a | (b << 8);
-                r.m = 0;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     r.h1[k] = k < S ? h1[k < S ? k : 0] : 0;
                     r.h2[k] = k < S ? h2[k < S ? k : 0] : 0;
-                    if (k < S) r.m |= m[k < S ? k : 0] << (8 * k);
                 }
+                r.stop = 0;
                 r.pad_ = 0;
                 mine = r;
             }
@@ -202,48 +196,43 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
         __syncthreads();
         // this CTA's best record, published for the cluster
         if (warp == 0) {
-            double xf = lane < nwarps ? rr[lane].f2 : inf_d();
+            uint64_t xk = lane < nwarps ? rr[lane].key : kNoSwap;
             int xq = lane < nwarps ? rr[lane].task : 0x7FFFFFFF;
-            const double own_f = xf;
+            const uint64_t own_k = xk;
             const int own_q = xq;
-            warp_argmin(xf, xq);
-            const int xw = __ffs(__ballot_sync(0xFFFFFFFFu, own_f == xf && own_q == xq)) - 1;
+            warp_argmin(xk, xq);
+            const int xw = __ffs(__ballot_sync(0xFFFFFFFFu, own_k == xk && own_q == xq)) - 1;
             if (lane == 0) cta_rec[round & 1] = rr[xw];
         }
         cluster.sync();
         // every warp reduces the cluster's records
-        double xf = inf_d();
+        uint64_t xk = kNoSwap;
         int xq = 0x7FFFFFFF;
         if (lane < csize) {
             const SwapRecord *remote = cluster.map_shared_rank(&cta_rec[round & 1], lane);
-            xf = remote->f2;
+            xk = remote->key;
             xq = remote->task;
         }
-        const double own_f = xf;
+        const uint64_t own_k = xk;
         const int own_q = xq;
-        warp_argmin(xf, xq);
-        const int xr = __ffs(__ballot_sync(0xFFFFFFFFu, own_f == xf && own_q == xq)) - 1;
-        if (xf < cur) {
+        warp_argmin(xk, xq);
+        if (xk != kNoSwap) {
+            const int xr = __ffs(__ballot_sync(0xFFFFFFFFu, own_k == xk && own_q == xq)) - 1;
             const SwapRecord w = *cluster.map_shared_rank(&cta_rec[round & 1], xr);
             const int a = w.ab & 0xFF, b = (w.ab >> 8) & 0xFF;
             row[w.s1] = (uint8_t)(5 * b);  // every CTA writes the swap itself
             row[w.s2] = (uint8_t)(5 * a);
-            for (int x = HEA_SITE_HIST ? tid : lane; x < NC; x += HEA_SITE_HIST ? blockDim.x : 32) {
-                const int k = x / (T * T), i = (x / T) % T, j = x % T;
-                const uint32_t h1 = w.h1[k], h2 = w.h2[k];
-                const int m = (w.m >> (8 * k)) & 0xFF;
-                const int ui = (int)((h2 >> (5 * i)) & 31u) - (int)((h1 >> (5 * i)) & 31u) + (i == b ? m : 0) -
-                               (i == a ? m : 0);
-                const int uj = (int)((h2 >> (5 * j)) & 31u) - (int)((h1 >> (5 * j)) & 31u) + (j == b ? m : 0) -
-                               (j == a ? m : 0);
-                cnt[x] += ((i == a) - (i == b)) * uj + ((j == a) - (j == b)) * ui;
-            }
-            if constexpr (HEA_SITE_HIST != 0) {
-                if (rank == 0) update_hist<L, true>(c, g.nbor, hist, w.s1, w.s2, a, b);
-                cluster.sync();  // the cluster's next proposals read the updated counts and histograms
-            } else {
-                __syncwarp();
-            }
+            const int32_t *cold = cnt2 + buf * NCP;
+            int32_t *cnew = cnt2 + (buf ^ 1) * NCP;
+            const auto after = [cold, &w, a, b](int k, int i, int j) {
+                return cold[(k * T + i) * T + j] + count_change<T>(w, a, b, k, i, j);
+            };
+            for (int x = tid; x < NC; x += blockDim.x) cnew[x] = after(x / (T * T), (x / T) % T, x % T);
+            delta_linear<T, S>(c, tab, after);
+            if (rank == 0) update_hist<L, true>(c, g.nbor, hist, w.s1, w.s2, a, b);
+            cluster.sync();  // the cluster's next proposals read the updated histograms; each CTA its table
+            buf ^= 1;
+            cur = __dadd_rn(cur, key_delta(xk));
             if (g.trace && rank == 0 && warp == 0 && accepts < g.trace_cap) {
                 if (lane == 0) {
                     AcceptRecord r;
@@ -251,15 +240,14 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
                     r.task = (uint32_t)xq;
                     r.s1 = w.s1;
                     r.s2 = w.s2;
-                    r.f2 = xf;
+                    r.f2 = cur;
                     g.trace[(size_t)sol * g.trace_cap + accepts] = r;
                 }
                 if (g.trace_counts) {
                     int32_t *dst = g.trace_counts + ((size_t)sol * g.trace_cap + accepts) * NC;
-                    for (int x = lane; x < NC; x += 32) dst[x] = cnt[x];
+                    for (int x = lane; x < NC; x += 32) dst[x] = cnew[x];
                 }
             }
-            cur = xf;
             miss = 0;
             ++accepts;
         } else {
@@ -269,14 +257,14 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
     }
     cluster.sync();  // every CTA's last reads of the row are done
     for (int s = lo + tid; s < hi; s += blockDim.x) row[s] = (uint8_t)(row[s] / 5);
-    if (rank == 0 && warp == 0)
-        for (int x = lane; x < NC; x += 32) gcnt[x] = cnt[x];
+    if (rank == 0)
+        for (int x = tid; x < NC; x += blockDim.x) gcnt[x] = cnt2[buf * NCP + x];
     unsigned long long ev = (unsigned long long)evals;
 #pragma unroll
     for (int o = 16; o; o >>= 1) ev += __shfl_xor_sync(0xFFFFFFFFu, ev, o);
     if (lane == 0 && ev) atomicAdd(&g.stats[1], ev);
     if (rank == 0 && tid == 0) {
-        g.f2[slot] = cur;
+        g.f2[slot] = fitness_of_counts<T, S>(c, cnt2 + buf * NCP);
         atomicAdd(&g.stats[0], (unsigned long long)round);
         atomicAdd(&g.stats[2], (unsigned long long)accepts);
         if (g.trace_len) g.trace_len[sol] = accepts;

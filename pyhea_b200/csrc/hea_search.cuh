@@ -87,8 +87,6 @@ struct GenArgs {
     int32_t generate;  // 1: draw a new occupancy; 0: recount the stored one
 };
 
-__device__ __forceinline__ double inf_d() { return __longlong_as_double(0x7FF0000000000000LL); }
-
 // ---------------------------------------------------------------------------
 // Fitness: f2 = sum_k w_k e_k; e_k accumulates d^2 with fma over the upper
 // triangle row by row (d_ii, then d_ij and d_ji for j > i); d = fma(-C', R, E).
@@ -121,167 +119,110 @@ __device__ __forceinline__ double fitness_of_counts(const SearchConst &c, const 
     return f2;
 }
 
-// Packed 5-bit species histogram of four neighbour ids.
-__device__ __forceinline__ uint32_t hist4(const int4 x, const uint8_t *occ5)
+// ---------------------------------------------------------------------------
+// The swap delta (how proposals are scored).  Swapping species a (at s1) and b
+// (at s2) changes the pair counts of shell k by dC_ij = sa_i u_j + sa_j u_i,
+// sa = e_a - e_b, where u_t = n2_t - n1_t + m ([t = b] - [t = a]); n1, n2 are
+// the species histograms of the two sites' shell-k neighbourhoods and m is how
+// often s2 is listed among s1's shell-k neighbours.  dC is zero outside rows and
+// columns a, b, so with d = E - R C (R symmetric) the change of
+// e_k = sum_ij d_ij^2 is exactly
+//     sum_t u_t (L_t + u_t Q_t) + (u_a - u_b)^2 Cq,
+//     L_t = -2 (G_at - G_bt),   G_it = R_it (d_it + d_ti),
+//     Q_t = 2 (R_at^2 + R_bt^2) for t != a, b,   Q_a = 4 R_aa^2,   Q_b = 4 R_bb^2,
+//     Cq  = 2 R_ab^2,
+// and f2 changes by D = sum_k w_k (that).  Each search keeps, per shell k and
+// ordered pair (a, b), the row {w L_t, w Q_t} (t < T), {w Cq, 0} in shared
+// memory (the delta table; Q and Cq depend on the structure only, L on the
+// counts and is rebuilt after every accepted swap) and scores a proposal by D
+// alone: O(T) terms per shell instead of the O(T^2) of a full fitness.
+// Fixed operation order (restated by the CPU oracle):
+//     Q   = w * (2 * (R_at * R_at + R_bt * R_bt)),  Q_a = w * (4 * (R_aa * R_aa)),
+//     Cq  = w * (2 * (R_ab * R_ab)),
+//     d_it = fma(-C, R_it, E_it),  G_it = R_it * (d_it + d_ti),  L = (-2 * w) * (G_at - G_bt),
+//     D = 0; per shell k: per t < T: D = fma(u_t, fma(u_t, Q_t, L_t), D); then D = fma((u_a - u_b)^2, Cq, D).
+// A round's best proposal (lowest D, lowest task on ties) is accepted iff D < 0;
+// the search's running f2 adds D, and the f2 a search stores at its end is
+// recomputed from the counts (fitness_of_counts).
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int delta_row(int T) { return (T + 1) | 1; }  // odd: lanes' rows spread over the banks
+__host__ __device__ constexpr int delta_entries(int T, int S) { return S * T * T * delta_row(T); }  // double2 entries
+
+// Structure constants of the table: w Q_t in .y of entries t < T, w Cq in .x
+// of entry T, for every (k, a, b), a != b.  Block-cooperative, no barrier.
+template <int T, int S>
+__device__ void delta_consts(const SearchConst &c, double2 *tab)
 {
-    return (1u << occ5[x.x]) + (1u << occ5[x.y]) + (1u << occ5[x.z]) + (1u << occ5[x.w]);
+    constexpr int R = delta_row(T);
+    for (int e = threadIdx.x; e < S * T * T * R; e += blockDim.x) {
+        const int t = e % R, ab = (e / R) % (T * T), k = e / (R * T * T);
+        const int a = ab / T, b = ab % T;
+        if (a == b || t > T) continue;
+        const double *Rk = c.R + k * T * T;
+        const double w = c.w[k];
+        if (t == T) {
+            tab[e].x = __dmul_rn(w, __dmul_rn(2.0, __dmul_rn(Rk[a * T + b], Rk[a * T + b])));
+        } else if (t == a || t == b) {
+            tab[e].y = __dmul_rn(w, __dmul_rn(4.0, __dmul_rn(Rk[t * T + t], Rk[t * T + t])));
+        } else {
+            const double p = __dmul_rn(Rk[a * T + t], Rk[a * T + t]), q = __dmul_rn(Rk[b * T + t], Rk[b * T + t]);
+            tab[e].y = __dmul_rn(w, __dmul_rn(2.0, __dadd_rn(p, q)));
+        }
+    }
 }
+
+// The count-dependent half of the table: w L_t in .x of entries t < T, from
+// the counts count_of(k, i, j) (symmetric in i, j).  Groups of T lanes of a
+// warp hold G_xt for x = 0..T-1 of one (shell, t); each lane takes the others'
+// G by shuffle and writes its row x against every y != x.  Warps call it
+// convergently (full-mask shuffles); no barrier inside.
+template <int T, int S, class CountOf>
+__device__ __forceinline__ void delta_linear(const SearchConst &c, double2 *tab, CountOf count_of)
+{
+    constexpr int R = delta_row(T), kGroups = 32 / T, kWarps = (S * T + kGroups - 1) / kGroups;
+    const int lane = threadIdx.x & 31, x = lane % T, grp = lane / T;
+    for (int w = threadIdx.x >> 5; w < kWarps; w += blockDim.x >> 5) {
+        const int g = w * kGroups + grp;  // shell k = g / T, column t = g % T
+        const bool on = grp < kGroups && g < S * T;
+        const int k = on ? g / T : 0, t = on ? g % T : 0;
+        const int xt = (k * T + x) * T + t, tx = (k * T + t) * T + x;
+        double G = 0.0, m2w = 0.0;
+        if (on) {
+            const double C = (double)count_of(k, x, t);
+            const double dxt = __fma_rn(-C, c.R[xt], c.E[xt]);
+            const double dtx = __fma_rn(-C, c.R[xt], c.E[tx]);
+            G = __dmul_rn(c.R[xt], __dadd_rn(dxt, dtx));
+            m2w = __dmul_rn(-2.0, c.w[k]);
+        }
+#pragma unroll
+        for (int y = 0; y < T; ++y) {
+            const double Gy = __shfl_sync(0xFFFFFFFFu, G, lane - x + y);
+            if (on && y != x) tab[((k * T + x) * T + y) * R + t].x = __dmul_rn(m2w, __dsub_rn(G, Gy));
+        }
+    }
+}
+
+__device__ __forceinline__ int field5(uint32_t h, int shift) { return (int)((h >> shift) & 31u); }
 
 __device__ __forceinline__ int count4(const int4 x, uint32_t v)
 {
     return ((uint32_t)x.x == v) + ((uint32_t)x.y == v) + ((uint32_t)x.z == v) + ((uint32_t)x.w == v);
 }
 
-// Histograms of shell k of both rows: h1 (s1's neighbours), h2 (s2's), and m =
-// the number of times s2 appears among s1's neighbours.  Fixed layouts issue
-// every load of the shell (both rows) before the first use.
-template <class L>
-__device__ __forceinline__ void shell_hist(const SearchConst &c, const int4 *__restrict__ r1,
-                                           const int4 *__restrict__ r2, const uint8_t *occ5, uint32_t s2, int k,
-                                           uint32_t &h1, uint32_t &h2, int &m)
-{
-    h1 = 0;
-    h2 = 0;
-    m = 0;
-    if constexpr (L::kRuntime) {
-        const int4 *a = r1 + c.off4[k], *b = r2 + c.off4[k];
-        for (int ch = 0; ch < c.chunks[k]; ++ch) {
-            const int4 x = __ldg(a + ch), y = __ldg(b + ch);
-            h1 += hist4(x, occ5);
-            h2 += hist4(y, occ5);
-            m += count4(x, s2);
-        }
-    } else {
-        constexpr int kMax = 7;
-        int4 x[kMax], y[kMax];
-        const int n = L::chunks(k), o = L::off(k);
-#pragma unroll
-        for (int ch = 0; ch < kMax; ++ch)
-            if (ch < n) {
-                x[ch] = __ldg(r1 + o + ch);
-                y[ch] = __ldg(r2 + o + ch);
-            }
-#pragma unroll
-        for (int ch = 0; ch < kMax; ++ch)
-            if (ch < n) {
-                h1 += hist4(x[ch], occ5);
-                h2 += hist4(y[ch], occ5);
-                m += count4(x[ch], s2);
-            }
-    }
-}
-
-// Row/column delta vector u of a shell for swapping species a (at s1) and b
-// (at s2): u_t = n2_t - n1_t + m([t==b] - [t==a]); the count change is
-// dC_ij = sa_i u_j + sa_j u_i with sa_i = [i==a] - [i==b].  Sentinel entries
-// add the same amount to field 0 of h1 and h2 and cancel here.
-template <int T>
-__device__ __forceinline__ void delta_vector(uint32_t h1, uint32_t h2, int m, int a, int b, int (&u)[T])
-{
-#pragma unroll
-    for (int t = 0; t < T; ++t) {
-        u[t] = (int)((h2 >> (5 * t)) & 31u) - (int)((h1 >> (5 * t)) & 31u);
-        u[t] += (t == b ? m : 0) - (t == a ? m : 0);
-    }
-}
-
-// e_k of shell k after adding dC (from u, a, b) to the counts cnt.
-template <int T>
-__device__ __forceinline__ double shell_error(const SearchConst &c, const int32_t *cnt, int k, const int (&u)[T],
-                                              int a, int b)
-{
-    double e = 0.0;
-#pragma unroll
-    for (int i = 0; i < T; ++i) {
-        const int sai = (i == a) - (i == b);
-        const int ii = (k * T + i) * T + i;
-        const double dii = __fma_rn(-(double)(cnt[ii] + 2 * sai * u[i]), c.R[ii], c.E[ii]);
-        e = __fma_rn(dii, dii, e);
-#pragma unroll
-        for (int j = i + 1; j < T; ++j) {
-            const int saj = (j == a) - (j == b);
-            const int ij = (k * T + i) * T + j, ji = (k * T + j) * T + i;
-            const double cp = (double)(cnt[ij] + sai * u[j] + saj * u[i]);
-            const double dij = __fma_rn(-cp, c.R[ij], c.E[ij]);
-            const double dji = __fma_rn(-cp, c.R[ij], c.E[ji]);
-            e = __fma_rn(dij, dij, e);
-            e = __fma_rn(dji, dji, e);
-        }
-    }
-    return e;
-}
-
-// Score one proposal: f2 of the counts after swapping s1 (species a) and s2 (b).
-// Returns the per-shell histograms so the accept step can apply the change.
-// kAhead (fixed layouts): issue the loads of every shell of both rows before
-// the first use -- one L2 round trip per proposal instead of one per shell, at
-// the cost of holding the whole rows in registers.
-template <int T, class L, bool kAhead = false>
-__device__ __forceinline__ double score_swap(const SearchConst &c, const int4 *__restrict__ nbor, const uint8_t *occ5,
-                                             const int32_t *cnt, uint32_t s1, uint32_t s2, int a, int b,
-                                             uint32_t (&h1)[L::S], uint32_t (&h2)[L::S], int (&m)[L::S])
-{
-    const int row4 = L::kRuntime ? c.row4 : L::kRow4;
-    const int4 *r1 = nbor + (size_t)s1 * row4;
-    const int4 *r2 = nbor + (size_t)s2 * row4;
-    if constexpr (kAhead && !L::kRuntime) {
-        constexpr int kRow = L::kRow4 > 0 ? L::kRow4 : 1;
-        int4 x[kRow], y[kRow];
-#pragma unroll
-        for (int ch = 0; ch < kRow; ++ch) {
-            x[ch] = __ldg(r1 + ch);
-            y[ch] = __ldg(r2 + ch);
-        }
-#pragma unroll
-        for (int k = 0; k < L::S; ++k) {
-            h1[k] = 0;
-            h2[k] = 0;
-            m[k] = 0;
-#pragma unroll
-            for (int ch = 0; ch < kRow; ++ch)
-                if (ch >= L::off(k) && ch < L::off(k) + L::chunks(k)) {
-                    h1[k] += hist4(x[ch], occ5);
-                    h2[k] += hist4(y[ch], occ5);
-                    m[k] += count4(x[ch], s2);
-                }
-        }
-    } else {
-        // shell by shell: the next shell's loads overlap this shell's fitness terms
-        double f2 = 0.0;
-#pragma unroll
-        for (int k = 0; k < L::S; ++k) {
-            shell_hist<L>(c, r1, r2, occ5, s2, k, h1[k], h2[k], m[k]);
-            int u[T];
-            delta_vector<T>(h1[k], h2[k], m[k], a, b, u);
-            f2 = __fma_rn(c.w[k], shell_error<T>(c, cnt, k, u, a, b), f2);
-        }
-        return f2;
-    }
-    double f2 = 0.0;
-#pragma unroll
-    for (int k = 0; k < L::S; ++k) {
-        int u[T];
-        delta_vector<T>(h1[k], h2[k], m[k], a, b, u);
-        f2 = __fma_rn(c.w[k], shell_error<T>(c, cnt, k, u, a, b), f2);
-    }
-    return f2;
-}
-
-// Score one proposal from the site histograms: H(s1) and H(s2) are the
-// neighbourhood histograms h1, h2 of score_swap, so only m (how often s2 is
-// listed among s1's shell-k neighbours) needs the table.  nbmask has bit
-// (n - s + N - 1) set for every table entry n of every site s; a clear bit for
-// s2 - s1 proves m = 0 in every shell, a set bit sends the lane to count s2
-// in s1's row.  Loads of H go through L2: the accept step updates H with
-// atomics.
-// p = hist[s1] and q = hist[s2], already loaded.
+// D of one proposal: s1 (species a, site histograms p), s2 (b, q).  On return
+// h1, h2 are the shell histograms with m folded in -- h1_k + (m << 5a), h2_k +
+// (m << 5b) -- so that u_t = field_t(h2_k) - field_t(h1_k); the fields stay
+// below 32 (n1_a + m <= Z_k because s1's list holds s2, of species b, m times;
+// likewise for h2).  nbmask has bit (n - s + N - 1) set for every table entry n
+// of every site s: a clear bit for s2 - s1 proves m = 0 in every shell, a set
+// bit sends the lane to count s2 in s1's row.
 template <int T, class L>
-__device__ __forceinline__ double score_swap_hist(const SearchConst &c, const int4 *__restrict__ nbor, const uint4 p,
-                                                  const uint4 q, const uint32_t *__restrict__ nbmask,
-                                                  const int32_t *cnt, uint32_t s1, uint32_t s2, int a, int b,
-                                                  uint32_t (&h1)[L::S], uint32_t (&h2)[L::S], int (&m)[L::S])
+__device__ __forceinline__ double score_delta(const SearchConst &c, const int4 *__restrict__ nbor,
+                                              const uint32_t *__restrict__ nbmask, const double2 *tab, const uint4 p,
+                                              const uint4 q, uint32_t s1, uint32_t s2, int a, int b,
+                                              uint32_t (&h1)[L::S], uint32_t (&h2)[L::S])
 {
-    constexpr int S = L::S;
+    constexpr int S = L::S, R = delta_row(T);
     const uint32_t d = s2 - s1 + (uint32_t)c.num_sites - 1u;
     const bool near = (__ldg(nbmask + (d >> 5)) >> (d & 31u)) & 1u;
     const uint32_t pv[3] = {p.x, p.y, p.z}, qv[3] = {q.x, q.y, q.z};
@@ -289,25 +230,35 @@ __device__ __forceinline__ double score_swap_hist(const SearchConst &c, const in
     for (int k = 0; k < S; ++k) {
         h1[k] = pv[k];
         h2[k] = qv[k];
-        m[k] = 0;
     }
+    const int a5 = 5 * a, b5 = 5 * b;
     if (near) {
         const int row4 = L::kRuntime ? c.row4 : L::kRow4;
         const int4 *r1 = nbor + (size_t)s1 * row4;
 #pragma unroll
         for (int k = 0; k < S; ++k) {
             const int o = L::kRuntime ? c.off4[k] : L::off(k), n = L::kRuntime ? c.chunks[k] : L::chunks(k);
-            for (int ch = 0; ch < n; ++ch) m[k] += count4(__ldg(r1 + o + ch), s2);
+            uint32_t m = 0;
+            for (int ch = 0; ch < n; ++ch) m += count4(__ldg(r1 + o + ch), s2);
+            h1[k] += m << a5;
+            h2[k] += m << b5;
         }
     }
-    double f2 = 0.0;
+    const double2 *row = tab + (a * T + b) * R;
+    double D = 0.0;
 #pragma unroll
     for (int k = 0; k < S; ++k) {
-        int u[T];
-        delta_vector<T>(h1[k], h2[k], m[k], a, b, u);
-        f2 = __fma_rn(c.w[k], shell_error<T>(c, cnt, k, u, a, b), f2);
+        const double2 *e = row + k * T * T * R;
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+            const double u = (double)(field5(h2[k], 5 * t) - field5(h1[k], 5 * t));
+            const double2 lq = e[t];
+            D = __fma_rn(u, __fma_rn(u, lq.y, lq.x), D);
+        }
+        const int v = field5(h2[k], a5) - field5(h1[k], a5) - field5(h2[k], b5) + field5(h1[k], b5);
+        D = __fma_rn((double)(v * v), e[T].x, D);
     }
-    return f2;
+    return D;
 }
 
 // After an accepted swap of s1 (species a -> b) and s2 (b -> a): update the
@@ -409,22 +360,27 @@ __device__ __forceinline__ bool draw_pair_hist(const SearchConst &c, uint32_t st
         s1, s2);
 }
 
-// Lexicographic (f2, task) minimum: the lowest task wins ties.
-__device__ __forceinline__ bool better(double f, int q, double bf, int bq) { return f < bf || (f == bf && q < bq); }
-
-// The warp's lexicographic (f, q) minimum in every lane, q >= 0.  f is an f2
-// (>= +0, or +inf for no proposal): such doubles order like their bit
-// patterns, so three 32-bit warp reductions (high word, low word among the
-// lanes holding the minimal high word, task among the lanes holding the
-// minimal f) give the exact minimum.
-__device__ __forceinline__ void warp_argmin(double &f, int &q)
+// Ordering key of a proposal's delta D: ~bits(D) for D < 0 (more negative,
+// smaller key), all ones for a proposal that does not improve (D >= 0) or for
+// no proposal.  The round's winner is the lexicographic (key, task) minimum.
+constexpr uint64_t kNoSwap = ~0ull;
+__device__ __forceinline__ uint64_t delta_key(double D)
 {
-    const unsigned long long bits = (unsigned long long)__double_as_longlong(f);
-    const uint32_t hi = (uint32_t)(bits >> 32), lo = (uint32_t)bits;
+    return D < 0.0 ? ~(uint64_t)__double_as_longlong(D) : kNoSwap;
+}
+__device__ __forceinline__ double key_delta(uint64_t key) { return __longlong_as_double((long long)~key); }
+__device__ __forceinline__ bool better(uint64_t k, int q, uint64_t bk, int bq) { return k < bk || (k == bk && q < bq); }
+
+// The warp's lexicographic (key, q) minimum in every lane, q >= 0: three
+// 32-bit warp reductions (high word, low word among the lanes holding the
+// minimal high word, task among the lanes holding the minimal key).
+__device__ __forceinline__ void warp_argmin(uint64_t &key, int &q)
+{
+    const uint32_t hi = (uint32_t)(key >> 32), lo = (uint32_t)key;
     const uint32_t mhi = __reduce_min_sync(0xFFFFFFFFu, hi);
     const uint32_t mlo = __reduce_min_sync(0xFFFFFFFFu, hi == mhi ? lo : 0xFFFFFFFFu);
     const uint32_t mq = __reduce_min_sync(0xFFFFFFFFu, (hi == mhi && lo == mlo) ? (uint32_t)q : 0xFFFFFFFFu);
-    f = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+    key = ((uint64_t)mhi << 32) | mlo;
     q = (int)mq;
 }
 
@@ -561,30 +517,41 @@ __global__ void __launch_bounds__(512, 1) generate_kernel(const SearchConst c, c
 // ---------------------------------------------------------------------------
 // The local parallel search (pyhea/cpp/accelerate.cpp:601-694): one CTA per
 // solution, one lane per task (lanes loop when tasks > blockDim).  Each round
-// every task scores one proposal against the same state; the block takes the
-// (f2, task) minimum and accepts it iff it is strictly below the current f2;
-// the search ends after `depth` rounds in a row without an accept.
+// every task scores one proposal against the same state (its delta D, see
+// score_delta); the block takes the (D, task) minimum and accepts it iff
+// D < 0; the search ends after `depth` rounds in a row without an accept.
 //
 // One block barrier per round: each warp publishes its best proposal (a
 // SwapRecord, double-buffered by round parity) before the barrier; after it
-// every warp reduces the records itself, writes the winning swap into the
-// shared occupancy (all threads write the same two bytes) and applies the count
-// change to its own copy of the counts, so no second barrier is needed before
-// the next round reads them.
-// Shared memory: occ_stride + 16 + nwarps * (4 * ncount_pad + 2 * sizeof(SwapRecord)).
+// every warp reduces the records itself and writes the winning swap into the
+// occupancy (all threads write the same two bytes).  On an accept the block
+// writes the counts after the swap into the other count buffer, rebuilds the
+// table's L half from them and updates the site histograms; a second barrier
+// publishes all three before the next round.
+//
+// Shared memory after the occupancy: the delta table, the records, two count
+// buffers (search_smem_tail).
 // ---------------------------------------------------------------------------
 struct SwapRecord {
-    double f2;
+    uint64_t key;           // delta_key of the proposal's D
     int32_t task;
     uint32_t s1, s2;
-    int32_t ab;          // species a | b << 8 before the swap
-    uint32_t h1[3], h2[3];
-    int32_t m;           // m_k in byte k
+    int32_t ab;             // species a | b << 8 before the swap
+    uint32_t h1[3], h2[3];  // shell histograms of both sites, m folded in (score_delta)
+    int32_t stop;           // record 0 of a round: the block stops after it (deadline)
     int32_t pad_;
 };
 static_assert(sizeof(SwapRecord) == 56, "SwapRecord layout");
 
 __host__ __device__ constexpr int mc_ncount_pad(int ncount) { return (ncount + 3) & ~3; }
+
+// Shared-memory bytes of a search after its occupancy: delta table, 2 * nwarps
+// swap records, two count buffers.
+__host__ __device__ constexpr size_t search_smem_tail(int T, int S, int nwarps)
+{
+    return (size_t)16 * delta_entries(T, S) + (size_t)2 * nwarps * sizeof(SwapRecord) +
+           (size_t)2 * 4 * mc_ncount_pad(S * T * T);
+}
 
 struct McTrace {
     AcceptRecord *records;  // trace_cap records for this search, or nullptr
@@ -593,50 +560,68 @@ struct McTrace {
 };
 
 struct McTally {
-    double f2;
+    double f2;                       // recomputed from the counts, or the running f2 when yielded
     int64_t rounds, accepts, evals;  // rounds run by this call
     int64_t round_end;               // round index the search continues from
     int miss;                        // consecutive rejections at round_end
+    int buf;                         // count buffer holding the final counts
     bool yielded;                    // stopped at the deadline before converging
 };
 
 // Where a search segment starts: a search stopped at a round boundary
-// continues from (round0, miss0) with the same occupancy, counts and f2 and
-// draws the same proposals as one that never stopped.
+// continues from (round0, miss0) with the same occupancy, counts and running
+// f2 and draws the same proposals as one that never stopped.
 struct McResume {
     int64_t round0;
     int miss0;
     unsigned long long deadline_ns;  // kYield: stop after the first round ending past this device time (0: never)
-    double tol2;                     // kYield: the search ends once f2 <= tol2 (< 0: never)
+    double tol2;                     // kYield: the search ends once its running f2 <= tol2 (< 0: never)
 };
 
-// Rounds of the local search on the staged state (occ5, the per-warp count
-// copies in cnt_all).  Every thread returns the same f2/rounds/accepts; evals
-// is this thread's count.  No barrier at entry; one per round.  occ5 may be
-// shared or global memory; every thread writes the accepted swap's bytes
-// itself, so its own later loads see them either way.  The draws read the
-// species from occ5.
-template <int T, class L, bool kAhead = false, bool kYield = false, bool kHist = false>
+// Count change dC_ij of shell k for the accepted swap in record w (a -> b at
+// s1, b -> a at s2): sa_i u_j + sa_j u_i with u from the record's histograms.
+template <int T>
+__device__ __forceinline__ int count_change(const SwapRecord &w, int a, int b, int k, int i, int j)
+{
+    const uint32_t h1 = w.h1[k], h2 = w.h2[k];
+    const int ui = field5(h2, 5 * i) - field5(h1, 5 * i), uj = field5(h2, 5 * j) - field5(h1, 5 * j);
+    return ((i == a) - (i == b)) * uj + ((j == a) - (j == b)) * ui;
+}
+
+// Delta table of a search starting from the counts in buffer 0 of cnt2
+// (the two halves of each entry are written by different threads, so one
+// barrier at the end covers both).  Block-wide.
+template <int T, int S>
+__device__ __forceinline__ void search_setup(const SearchConst &c, const int32_t *cnt2, double2 *tab)
+{
+    delta_consts<T, S>(c, tab);
+    delta_linear<T, S>(c, tab, [cnt2](int k, int i, int j) { return cnt2[(k * T + i) * T + j]; });
+    __syncthreads();
+}
+
+// Rounds of the local search on the staged state: occupancy occ5, counts in
+// buffer 0 of cnt2, the delta table tab (search_setup), running f2 `cur`.
+// Every thread returns the same tally; evals is this thread's count.  No
+// barrier at entry.  occ5 may be shared or global memory; every thread writes
+// the accepted swap's bytes itself, so its own later loads see them either
+// way.  The draws read the species from occ5; proposals are scored from the
+// site histograms `hist`, which an accept updates.
+template <int T, class L, bool kYield = false>
 __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *__restrict__ nbor, uint8_t *occ5,
-                                             int32_t *cnt_all, SwapRecord *rec, uint32_t stream, double cur,
-                                             int tasks, int depth, int64_t max_rounds, McTrace tr,
-                                             McResume rs = McResume{0, 0, 0ull, -1.0}, uint4 *hist = nullptr,
-                                             const uint32_t *nbmask = nullptr)
+                                             int32_t *cnt2, double2 *tab, SwapRecord *rec, uint32_t stream,
+                                             double cur, int tasks, int depth, int64_t max_rounds, McTrace tr,
+                                             McResume rs, uint4 *hist, const uint32_t *nbmask)
 {
     constexpr int S = L::S, NC = S * T * T, NCP = mc_ncount_pad(NC);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    // kHist: one shared copy of the counts, updated by the whole block on an
-    // accept (the barrier after the histogram update publishes both); the
-    // gather form keeps one copy per warp so an accept needs no barrier
-    int32_t *cnt = kHist ? cnt_all : cnt_all + warp * NCP;
-    int miss = rs.miss0;
+    int miss = rs.miss0, buf = 0;
     int64_t round = rs.round0, accepts = 0, evals = 0;
     bool yielded = false;
     while (miss < depth && round < max_rounds && !(kYield && cur <= rs.tol2)) {
         SwapRecord *rr = rec + (round & 1) * nwarps;
         SwapRecord &mine = rr[warp];  // this warp's best proposal of the round
         if (lane == 0) {
-            mine.f2 = inf_d();
+            mine.key = kNoSwap;
             mine.task = 0x7FFFFFFF;
         }
         __syncwarp();
@@ -646,94 +631,82 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
             uint32_t s1 = 0, s2 = 0;
             const bool ok = q < tasks && draw_pair(c, stream, (uint32_t)round, (uint32_t)q, occ5, s1, s2);
             __syncwarp();  // lanes that needed more draws rejoin before scoring
-            double f = inf_d();
+            uint64_t key = kNoSwap;
             uint32_t h1[S], h2[S];
-            int m[S], a = 0, b = 0;
+            int a = 0, b = 0;
             if (ok) {
                 ++evals;
-                if constexpr (kHist) {
-                    a = occ5[s1] / 5;
-                    b = occ5[s2] / 5;
-                    f = score_swap_hist<T, L>(c, nbor, __ldcg(hist + s1), __ldcg(hist + s2), nbmask, cnt, s1, s2, a, b,
-                                              h1, h2, m);
-                } else {
-                    a = occ5[s1] / 5;
-                    b = occ5[s2] / 5;
-                    f = score_swap<T, L, kAhead>(c, nbor, occ5, cnt, s1, s2, a, b, h1, h2, m);
-                }
+                a = occ5[s1] / 5;
+                b = occ5[s2] / 5;
+                key = delta_key(score_delta<T, L>(c, nbor, nbmask, tab, __ldcg(hist + s1), __ldcg(hist + s2), s1, s2,
+                                                  a, b, h1, h2));
             }
-            double wf = f;
-            int wq = ok ? q : 0x7FFFFFFF;
-            warp_argmin(wf, wq);
+            uint64_t wk = key;
+            int wq = key != kNoSwap ? q : 0x7FFFFFFF;
+            warp_argmin(wk, wq);
             // the lane holding the pass minimum folds it into the warp's record
-            if (ok && wq == q && better(wf, wq, mine.f2, mine.task)) {
+            if (key != kNoSwap && wq == q && better(wk, wq, mine.key, mine.task)) {
                 SwapRecord r;
-                r.f2 = wf;
+                r.key = wk;
                 r.task = wq;
                 r.s1 = s1;
                 r.s2 = s2;
                 r.ab = a | (b << 8);
-                r.m = 0;
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     r.h1[k] = k < S ? h1[k < S ? k : 0] : 0;
                     r.h2[k] = k < S ? h2[k < S ? k : 0] : 0;
-                    if (k < S) r.m |= m[k < S ? k : 0] << (8 * k);
                 }
+                r.stop = 0;
                 r.pad_ = 0;
                 mine = r;
             }
             __syncwarp();
         }
         // the stop decision travels in warp 0's record (read by all after the barrier)
-        if (kYield && tid == 0) rr[0].pad_ = (rs.deadline_ns && global_ns() >= rs.deadline_ns) ? 1 : 0;
+        if (kYield && tid == 0) rr[0].stop = (rs.deadline_ns && global_ns() >= rs.deadline_ns) ? 1 : 0;
         __syncthreads();
-        const bool stop = kYield && rr[0].pad_ != 0;
+        const bool stop = kYield && rr[0].stop != 0;
         // every warp reduces the records of all warps
-        double xf = lane < nwarps ? rr[lane].f2 : inf_d();
+        uint64_t xk = lane < nwarps ? rr[lane].key : kNoSwap;
         int xq = lane < nwarps ? rr[lane].task : 0x7FFFFFFF;
-        const double own_f = xf;
+        const uint64_t own_k = xk;
         const int own_q = xq;
-        warp_argmin(xf, xq);
-        // the record holding the minimum (tasks of finite records are distinct)
-        const int xw = __ffs(__ballot_sync(0xFFFFFFFFu, own_f == xf && own_q == xq)) - 1;
-        if (xf < cur) {
+        warp_argmin(xk, xq);
+        if (xk != kNoSwap) {
+            // the record holding the minimum (tasks of records are distinct)
+            const int xw = __ffs(__ballot_sync(0xFFFFFFFFu, own_k == xk && own_q == xq)) - 1;
             const SwapRecord &w = rr[xw];
             const int a = w.ab & 0xFF, b = (w.ab >> 8) & 0xFF;
             occ5[w.s1] = (uint8_t)(5 * b);  // same bytes from every thread
             occ5[w.s2] = (uint8_t)(5 * a);
-            for (int x = kHist ? tid : lane; x < NC; x += kHist ? blockDim.x : 32) {
-                const int k = x / (T * T), i = (x / T) % T, j = x % T;
-                const uint32_t h1 = w.h1[k], h2 = w.h2[k];
-                const int m = (w.m >> (8 * k)) & 0xFF;
-                const int ui = (int)((h2 >> (5 * i)) & 31u) - (int)((h1 >> (5 * i)) & 31u) + (i == b ? m : 0) -
-                               (i == a ? m : 0);
-                const int uj = (int)((h2 >> (5 * j)) & 31u) - (int)((h1 >> (5 * j)) & 31u) + (j == b ? m : 0) -
-                               (j == a ? m : 0);
-                cnt[x] += ((i == a) - (i == b)) * uj + ((j == a) - (j == b)) * ui;
-            }
-            if constexpr (kHist) {
-                update_hist<L, false>(c, nbor, hist, w.s1, w.s2, a, b);
-                __syncthreads();  // next round's proposals read the updated counts and histograms
-            } else {
-                __syncwarp();
-            }
+            const int32_t *cold = cnt2 + buf * NCP;
+            int32_t *cnew = cnt2 + (buf ^ 1) * NCP;
+            const auto after = [cold, &w, a, b](int k, int i, int j) {
+                return cold[(k * T + i) * T + j] + count_change<T>(w, a, b, k, i, j);
+            };
+            for (int x = tid; x < NC; x += blockDim.x) cnew[x] = after(x / (T * T), (x / T) % T, x % T);
+            delta_linear<T, S>(c, tab, after);
+            update_hist<L, false>(c, nbor, hist, w.s1, w.s2, a, b);
+            const double D = key_delta(xk);
+            __syncthreads();  // next round's proposals read the new table and histograms
+            buf ^= 1;
+            cur = __dadd_rn(cur, D);
             if (tr.records && warp == 0 && accepts < tr.cap) {
                 if (lane == 0) {
                     AcceptRecord r;
                     r.round = (uint32_t)round;
                     r.task = (uint32_t)xq;
-                    r.s1 = w.s1;
-                    r.s2 = w.s2;
-                    r.f2 = xf;
+                    r.s1 = rr[xw].s1;
+                    r.s2 = rr[xw].s2;
+                    r.f2 = cur;
                     tr.records[accepts] = r;
                 }
                 if (tr.counts) {
                     int32_t *dst = tr.counts + accepts * NC;
-                    for (int x = lane; x < NC; x += 32) dst[x] = cnt[x];
+                    for (int x = lane; x < NC; x += 32) dst[x] = cnew[x];
                 }
             }
-            cur = xf;
             miss = 0;
             ++accepts;
         } else {
@@ -746,7 +719,8 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
         }
     }
     __syncthreads();
-    return McTally{cur, round - rs.round0, accepts, evals, round, miss, yielded};
+    const double f2 = yielded ? cur : fitness_of_counts<T, S>(c, cnt2 + buf * NCP);
+    return McTally{f2, round - rs.round0, accepts, evals, round, miss, buf, yielded};
 }
 
 // Slot row (species bytes) -> 5*species in shared memory (16-byte vectors).
@@ -802,21 +776,20 @@ __device__ __forceinline__ void add_tally(const McTally &t, unsigned long long *
     }
 }
 
-#ifndef HEA_SITE_HIST
-#define HEA_SITE_HIST 1  // score proposals from the site histograms (0: gather the neighbours' species)
-#endif
 #ifndef HEA_MC_MIN_BLOCKS
 #define HEA_MC_MIN_BLOCKS 2  // resident 512-thread blocks per SM the register budget aims for
 #endif
+// Shared memory: occ_stride + 16 + search_smem_tail(T, S, nwarps).
 template <int T, class L>
 __global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const SearchConst c, const McArgs g)
 {
     constexpr int S = L::S, NC = S * T * T, NCP = mc_ncount_pad(NC);
     extern __shared__ __align__(16) uint8_t smem[];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const int tid = threadIdx.x, nwarps = blockDim.x >> 5;
     uint8_t *occ5 = smem;
-    int32_t *cnt_all = reinterpret_cast<int32_t *>(smem + c.occ_stride + 16);
-    SwapRecord *rec = reinterpret_cast<SwapRecord *>(cnt_all + nwarps * NCP);  // [2][nwarps]
+    double2 *tab = reinterpret_cast<double2 *>(smem + c.occ_stride + 16);
+    SwapRecord *rec = reinterpret_cast<SwapRecord *>(tab + delta_entries(T, S));  // [2][nwarps]
+    int32_t *cnt2 = reinterpret_cast<int32_t *>(rec + 2 * nwarps);                // [2][NCP]
 
     const int slot = g.order[blockIdx.x];
     const uint32_t stream = (g.mc_call << 16) | (uint32_t)blockIdx.x;
@@ -824,10 +797,10 @@ __global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const Search
     int32_t *gcnt = g.cnt + (size_t)slot * NC;
 
     stage_occupancy(c, gocc, occ5);
-    for (int x = lane; x < NC; x += 32) cnt_all[warp * NCP + x] = gcnt[x];
+    for (int x = tid; x < NC; x += blockDim.x) cnt2[x] = gcnt[x];
     __syncthreads();
     if (tid == 0) occ5[c.num_sites] = 0;  // sentinel (occ_stride may end exactly at n)
-    __syncthreads();
+    search_setup<T, S>(c, cnt2, tab);
 
     McTrace tr{nullptr, nullptr, 0};
     if (g.trace) {
@@ -835,13 +808,12 @@ __global__ void __launch_bounds__(512, HEA_MC_MIN_BLOCKS) mc_kernel(const Search
         tr.counts = g.trace_counts ? g.trace_counts + (size_t)blockIdx.x * g.trace_cap * NC : nullptr;
         tr.cap = g.trace_cap;
     }
-    const McTally t = mc_rounds<T, L, false, false, HEA_SITE_HIST != 0>(
-        c, g.nbor, occ5, cnt_all, rec, stream, g.f2[slot], g.tasks, g.depth, g.max_rounds, tr,
-        McResume{0, 0, 0ull, -1.0}, g.hist ? g.hist + (size_t)slot * c.num_sites : nullptr, g.nbmask);
+    const McTally t = mc_rounds<T, L>(c, g.nbor, occ5, cnt2, tab, rec, stream, g.f2[slot], g.tasks, g.depth,
+                                      g.max_rounds, tr, McResume{0, 0, 0ull, -1.0},
+                                      g.hist + (size_t)slot * c.num_sites, g.nbmask);
 
     unstage_occupancy(c, occ5, gocc);
-    if (warp == 0)
-        for (int x = lane; x < NC; x += 32) gcnt[x] = cnt_all[x];
+    for (int x = tid; x < NC; x += blockDim.x) gcnt[x] = cnt2[t.buf * NCP + x];
     add_tally(t, g.stats);
     if (tid == 0) {
         g.f2[slot] = t.f2;

@@ -115,15 +115,50 @@ def test_mc_counts_match_recount_after_every_accept():
     res = pr.mc(11, 5, occ0, tasks=16, depth=4, trace_cap=5000, trace_counts=True)
     assert res["accepts"] > 10
     occ = occ0.copy()
-    last = np.inf
+    last = pr.f2(pr.recount(occ0))
     for (rnd, task, s1, s2, f2), cnt in zip(res["trace"], res["trace_counts"]):
         occ[s1], occ[s2] = occ[s2], occ[s1]
         np.testing.assert_array_equal(cnt, pr.recount(occ))
-        assert f2 == pr.f2(cnt) and f2 < last
+        # the running f2 (sum of the accepted deltas) tracks a recount's to rounding
+        assert abs(f2 - pr.f2(cnt)) <= 1e-12 * pr.f2(cnt) and f2 < last
         last = f2
     np.testing.assert_array_equal(occ, res["occ"])
     np.testing.assert_array_equal(res["counts"], pr.recount(occ))
+    assert res["f2"] == pr.f2(res["counts"])
     assert res["evals"] <= res["rounds"] * 16
+
+
+@pytest.mark.parametrize("lat,cell,species,shell_set", [
+    (L.FCC, 4, (100, 156), L.SHELLS_REFERENCE),
+    (L.BCC, 5, (40, 42, 42, 42, 42, 42), L.SHELLS_REFERENCE),
+    (L.FCC, 3, (20, 22, 22, 22, 22), L.SHELLS_FCC_TRUE3),
+    (L.BCC, 4, (40, 44, 44), L.SHELLS_REFERENCE),
+    (L.FCC, 4, (64, 64, 64, 64), L.SHELLS_FCC_TRUE3),
+])
+def test_delta_is_the_change_of_fitness(lat, cell, species, shell_set):
+    """The scoring contract's D equals f2(counts after the swap) - f2(counts before) -- the
+    reference's full fitness of the swapped state minus the current one (accelerate.cpp:555-569)
+    -- to rounding, for random states and swaps, including neighbouring pairs (m > 0)."""
+    st = W.small_case(lattice=lat, cell=cell, species=species, shell_set=shell_set, seed=3)
+    nbor, ss = st.neighbors()
+    pr = ho.Problem(nbor, ss, st.species, st.weight, st.target)
+    rng = np.random.default_rng(5)
+    near = 0
+    for trial in range(300):
+        occ = pr.generate(trial, 0, 0)
+        C = pr.recount(occ)
+        f0 = pr.f2(C)
+        s1 = int(rng.integers(pr.num_sites))
+        cand = nbor[s1] if trial % 3 == 0 else rng.integers(pr.num_sites, size=8)
+        s2 = next((int(x) for x in cand if occ[int(x)] != occ[s1]), None)
+        if s2 is None:
+            continue
+        near += int(s2 in nbor[s1])
+        f1 = pr.f2(pr.swap_counts(occ, C, s1, s2))
+        D = pr.delta(occ, C, s1, s2)
+        assert abs(D - (f1 - f0)) <= 1e-13 * max(f0, f1), (trial, D, f1 - f0)
+        assert (D < 0) == (f1 < f0) or abs(f1 - f0) <= 1e-13 * f0
+    assert near > 20
 
 
 def test_hcs_sorted_deterministic_and_improving():
