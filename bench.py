@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Swap-evaluation throughput of the SRO-targeted swap search on B200.
 
-Workload (default): the plain GPU configuration -- BCC 20x20x20 (16000 sites,
+Headline (default): the plain GPU configuration -- BCC 20x20x20 (16000 sites,
 8/6/12 shells), 5 species x 3200 atoms, seeded synthetic target alpha
 (U(-0.15, 0.15), zero row sums), weights [4, 1, 0.5], 256 solutions x 512
 tasks, 50 iterations, converge depth 20.  One step = one whole search
@@ -14,18 +14,45 @@ tasks, 50 iterations, converge depth 20.  One step = one whole search
          (hea_run_local_parallel_hcs): neighbour table and inputs copied from
          pinned memory and the population read back inside the timed region
   roofline  the local-search kernel: algorithmic bytes (2 sum Z (4 B id + 1 B
-         species) + 2 B per evaluation) over its CUDA-event time, against the
-         measured HBM copy bandwidth
+         species) + 2 B per evaluation) over its CUDA-event time against the
+         measured HBM copy bandwidth (the normalisation every line uses), and
+         the two ceilings that bind the kernel: L2 bytes per evaluation (ncu)
+         against an L2 read peak measured here by the library's own probe
+         kernel (l2_frac), and warp instructions per evaluation (ncu) against
+         the SMs' issue rate at the sampled SM clock (issue_frac)
   cpu_baseline  the reference CPU engine (oracle/_ref) on a bounded sample
+  dropin_e2e  the pybind11 drop-in called as pyhea/model/opt.py:89-90 calls it
+         (nested Python lists, per-iteration log on), end to end
 
+At one GPU the line also carries the other configurations, each measured here:
+  batched   the mixed 64-structure batch on the persistent kernel against the
+            same structures searched one plain plan at a time (same seeds, same
+            results), with its own roofline
+  serving   a Poisson request stream through the serving loop at the stated
+            request size (64 solutions x 256 tasks): sustained requests/s,
+            latency p50/p90/p99 and by request size
+  large     FCC 100^3 (4,000,000 sites): iterations of the uncapped search
+  time_to_tol  wall time until the best fitness reaches 1e-3 (PyHEA's default
+            threshold) on the plain GPU and CPU structures, plus looser tolerances
+
+--workload batched|large|serving|plain_cpu prints that configuration's own line.
 --impl reference times the reference CPU engine alone (rank 0) on the same
 workload and prints the same line with "impl": "reference".
+
+--case plain|batch|large runs one small fixed case for a profiler capture and
+prints its statistics (rounds, evaluations, accepts, device time) as JSON:
+  plain [--iters 1]            one search of the plain GPU structure
+  batch [--count 16] [--iters 1]  the `count` largest structures of the mixed
+                               batch, one batched run
+  large [--cell 40] [--rounds 500]  one local search of an FCC cell^3 supercell
+                               on the HBM cluster path (32 solutions x 4096 tasks)
 Multi-GPU: replicas -- every rank searches its own copy of the workload with
 its own seeds; no collective on the data path.
 """
 import argparse
 import datetime
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -37,13 +64,21 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per swap evaluation of the dominant
-# kernel, from one ncu capture each, reported per launch as roofline.traffic, scaled by the
-# evaluations of the bench's launches: mc_kernel on the plain GPU workload, 164.5 MB over its first
-# local-search launch of 203.7 M evaluations (python -m pyhea_b200.cases plain --iters 1);
-# batch_kernel on the 64-structure batch, 152.5 GB over a launch of 631.3 M evaluations
-# (python -m pyhea_b200.cases batch --count 64 --iters 1).
-DRAM_BYTES_PER_EVAL = {"plain_gpu": 164.5e6 / 203.7e6, "batched": 152.467e9 / 631.335e6}
+# Per-evaluation counters of the dominant kernel from one ncu capture each (per launch, so they
+# scale to the bench's launches by their evaluations):
+#   dram   dram__bytes_read.sum + dram__bytes_write.sum      -> roofline.traffic
+#   l2     lts__t_sectors_srcunit_tex.sum x 32 B              -> roofline.l2_frac
+#   inst   smsp__inst_executed.sum (warp instructions)        -> roofline.issue_frac
+# mc_kernel<5, Shells<2,2,3>>: the first local-search launch of `python bench.py --case plain
+# --iters 1` (203.72 M evaluations): 163.78 MB DRAM, 433.1 M L2 sectors, 3.808 G warp instructions.
+# batch_kernel: one launch of `python bench.py --case batch --count 64 --iters 1`.
+KERNEL_COUNTERS = {
+    "plain_gpu": {"dram": 163.78e6 / 203.72e6, "l2": 2.126 * 32.0, "inst": 18.69,
+                  "capture": "mc_kernel, first local-search launch of bench.py --case plain --iters 1"},
+    "batched": {"dram": 152.467e9 / 631.335e6, "l2": None, "inst": None,
+                "capture": "batch_kernel, bench.py --case batch --count 64 --iters 1"},
+}
+L2_PROBE_BYTES = 32 << 20  # fits in L2 (126 MB) with room to spare
 
 
 def parse_args():
@@ -56,12 +91,19 @@ def parse_args():
                     default="plain_gpu")
     ap.add_argument("--serve-rate", type=float, default=200.0, help="serving: Poisson arrival rate, requests/s")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving: arrival window, seconds")
-    ap.add_argument("--slice-ms", type=float, default=40.0,
-                    help="serving: time slice of one server step (measured at 200 req/s: 40 ms best p99 of 2-80)")
-    ap.add_argument("--large-rounds", type=int, default=4000,
-                    help="large workload: cap on rounds per local search (the uncapped search runs for hours)")
+    ap.add_argument("--serve-solutions", type=int, default=64, help="serving: solutions per request")
+    ap.add_argument("--serve-iters", type=int, default=10, help="serving: iterations per request (tolerance ends it)")
+    ap.add_argument("--slice-ms", type=float, default=40.0, help="serving: time slice of one server step")
+    ap.add_argument("--large-iters", type=int, default=1, help="large: iterations of the uncapped search")
+    ap.add_argument("--tol-iters", type=int, default=400, help="time_to_tol: iteration cap")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="headline line only (no batched/serving/large)")
     ap.add_argument("--cpu-procs", type=int, default=0, help="reference processes (0: all host cores)")
+    ap.add_argument("--case", choices=["plain", "batch", "large"], help="one small case for a profiler capture")
+    ap.add_argument("--iters", type=int, default=1, help="--case plain/batch: iterations")
+    ap.add_argument("--count", type=int, default=16, help="--case batch: structures")
+    ap.add_argument("--cell", type=int, default=40, help="--case large: FCC cell edge")
+    ap.add_argument("--rounds", type=int, default=500, help="--case large: round cap")
     return ap.parse_args()
 
 
@@ -115,6 +157,7 @@ class ClockSampler:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+        return self
 
     def stop(self):
         if self.proc is None:
@@ -141,6 +184,37 @@ class ClockSampler:
         loaded = [r[0] for r in rows if r[0] > 0.5 * r[1]] or [r[0] for r in rows]
         return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
                 "samples": len(rows)}
+
+
+def sm_count():
+    import torch
+
+    return torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+
+
+def roofline_of(kernel, counters, evals, kernel_s, bytes_per_eval, launches, clocks, l2_peak, sms):
+    """Roofline object of one kernel: the algorithmic-byte normalisation against HBM, plus the L2 and
+    issue ceilings from the kernel's ncu counters per evaluation (see KERNEL_COUNTERS)."""
+    peak, peak_kind = measured_peaks()
+    rate = evals / kernel_s if kernel_s > 0 else 0.0
+    achieved = rate * bytes_per_eval / 1e9
+    out = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+           "kernel": kernel, "bytes_per_eval": bytes_per_eval, "peak_kind": peak_kind,
+           "traffic": counters["dram"] * evals / launches if counters.get("dram") and launches else None,
+           "algorithmic_bytes_per_launch": evals * bytes_per_eval / launches if launches else None,
+           "counters_from": counters["capture"]}
+    if counters.get("l2") and l2_peak:
+        l2_gbs = rate * counters["l2"] / 1e9
+        out["l2"] = {"bytes_per_eval": counters["l2"], "achieved_gbs": l2_gbs, "peak_gbs": l2_peak,
+                     "peak_kind": "measured (hea_l2_read_probe, 32 MiB read through L2)"}
+        out["l2_frac"] = l2_gbs / l2_peak
+    if counters.get("inst") and sms:
+        mhz = (clocks or {}).get("sm_mhz") or 1965.0
+        peak_inst = sms * 4 * mhz * 1e6  # one warp instruction per SM sub-partition per cycle
+        out["issue"] = {"warp_inst_per_eval": counters["inst"], "achieved_per_s": rate * counters["inst"],
+                        "peak_per_s": peak_inst, "sm_mhz": mhz}
+        out["issue_frac"] = rate * counters["inst"] / peak_inst
+    return out
 
 
 def cpu_reference_sample(st, nbor, sizes, procs, nnet_per_proc=5, step=1):
@@ -171,7 +245,7 @@ def run_reference(args):
                           "batched reference lines"}[args.workload]
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return 0
-    from pyhea_b200 import workloads as W
+    from pyhea_b200 import workloads as W  # numpy only: maps none of this build's libraries
 
     structs = W.batched(seed=0) if args.workload == "batched" else [workload(args.workload)]
     procs = args.cpu_procs or host_cores()
@@ -181,7 +255,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_accelerate.so was not built"}))
         return 0
     pool = RefPool(procs)
-    nnet = max(1, 2)
+    nnet = 2
     total_evals, total_s = 0.0, 0.0
     try:
         for i in range(args.warmup + args.steps):
@@ -212,18 +286,20 @@ def run_reference(args):
     return 0
 
 
-def run_batched(args):
-    """Mixed-size batch: 64 structures (FCC/BCC, edge 6..30, 3-6 species, Dirichlet(2)
-    compositions), 64 solutions x 256 tasks, 10 iterations, depth 10.  value = swap
-    evaluations/s of the batched persistent kernel; plain = the same structures searched one
-    structure per launch sequence (device-resident plans), same seeds, same results."""
+# ---------------------------------------------------------------------------
+# Batched: the mixed 64-structure batch
+# ---------------------------------------------------------------------------
+def measure_batched(steps, warmup, l2_peak=None):
+    """64 structures (FCC/BCC, edge 6..30, 3-6 species, Dirichlet(2) compositions), 64 solutions x
+    256 tasks, 10 iterations, depth 10.  value = swap evaluations/s of the batched persistent kernel;
+    plain = the same structures searched one structure per launch sequence (device-resident plans,
+    CTA size autotuned), same seeds, same results."""
     import numpy as np
     import torch
 
     import pyhea_b200 as hb
     from pyhea_b200 import workloads as W
 
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     structs = W.batched(seed=0)
     problems = [st.problem(device=True) for st in structs]
     params = [dict(num_solutions=st.P, total_iter=st.I, parallel_task=st.Q, converge_depth=st.D) for st in structs]
@@ -233,28 +309,26 @@ def run_batched(args):
     tuned = batch.autotune()  # launch configuration timed on full runs, before the warm-up
     plans = [hb.Plan(pb, st.P, st.I, st.Q, st.D, autotune=True) for pb, st in zip(problems, structs)]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    for w in range(args.warmup):
+    for w in range(warmup):
         batch.run(seeds(w))
     b_ms, b_ev, p_ms, p_ev = 0.0, 0, 0.0, 0
-    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
-    sampler.start()
-    for k in range(args.steps):
+    sampler = ClockSampler(torch.cuda.current_device()).start()
+    for k in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
-        s = batch.run(seeds(args.warmup + k))
+        s = batch.run(seeds(warmup + k))
         b_ms += s["gpu_ms"]
         b_ev += s["evals"]
     clocks = sampler.stop()
     evals_of = [int(t[1]) for t in batch.tallies()]  # per structure, last step
-    for k in range(args.steps):
+    for k in range(steps):
         for i, plan in enumerate(plans):
             flush.zero_()
             torch.cuda.synchronize()
-            s = plan.run(seeds(args.warmup + k)[i])
+            s = plan.run(seeds(warmup + k)[i])
             p_ms += s["gpu_ms"]
             p_ev += s["evals"]
-    # same seeds, same results: the last step of each path
-    same = 0
+    same = 0  # same seeds, same results: the last step of each path
     for i, plan in enumerate(plans):
         same += int(np.array_equal(batch.read(i)[0], plan.read()[0]))
     for plan in plans:
@@ -272,133 +346,139 @@ def run_batched(args):
     h2d = sum(pb.nbor.nbytes + pb.shell_sizes.nbytes + pb.species.nbytes + pb.weight.nbytes + pb.target_sro.nbytes
               for pb in pinned)
     d2h = sum(st.P * (st.num_sites + 8) for st in structs)
-    for k in range(args.steps):
+    for k in range(steps):
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         eb = hb.Batch(pinned, params)
-        s = eb.run(seeds(args.warmup + k))
+        s = eb.run(seeds(warmup + k))
         for i in range(len(structs)):
             eb.read(i)
         eb.close()
         e2e_s += time.perf_counter() - t0
         e2e_ev += s["evals"]
 
-    # roofline of the persistent kernel: each structure's algorithmic bytes per evaluation
-    # (BCC 8/6/12 262 B, FCC 12/6/24 422 B) weighted by its evaluations in the batch's last step, over
-    # the batch's device time
-    peak, peak_kind = measured_peaks()
-    alg_bytes = sum(e * st.evals_bytes() for e, st in zip(evals_of, structs)) / max(1, sum(evals_of)) * b_ev
-    achieved = alg_bytes / (b_ms / 1000.0) / 1e9
-    line = {"metric": "swap_evals_per_sec", "value": value, "unit": "swap-evals/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": b_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "batched: 64 mixed FCC/BCC structures", "sites_total": int(sum(st.num_sites for st in structs)),
-                       "solutions": 64, "parallel_task": 256, "total_iter": 10, "converge_depth": 10,
+    # roofline: each structure's algorithmic bytes per evaluation (BCC 8/6/12 262 B, FCC 12/6/24
+    # 422 B) weighted by its evaluations in the last step
+    bpe = sum(e * st.evals_bytes() for e, st in zip(evals_of, structs)) / max(1, sum(evals_of))
+    roof = roofline_of("batch_kernel (persistent job engine)", KERNEL_COUNTERS["batched"], b_ev, b_ms / 1000.0,
+                       bpe, steps, clocks, l2_peak, sm_count())
+    return {"value": value, "unit": "swap-evals/s", "steps": steps, "warmup": warmup, "ms_per_step": b_ms / steps,
+            "config": {"workload": "batched: 64 mixed FCC/BCC structures",
+                       "sites_total": int(sum(st.num_sites for st in structs)), "solutions": 64,
+                       "parallel_task": 256, "total_iter": 10, "converge_depth": 10,
                        "l2": "flushed between timed steps (256 MiB write)", "batch_launch": tuned},
-            "plain": {"value": plain, "ms_per_step": p_ms / args.steps, "evals_per_step": p_ev / args.steps},
+            "plain": {"value": plain, "ms_per_step": p_ms / steps, "evals_per_step": p_ev / steps},
             "speedup_vs_plain": value / plain, "identical_structures": same, "structures": len(structs),
-            "evals_per_step": b_ev / args.steps, "clocks": clocks,
+            "evals_per_step": b_ev / steps, "clocks": clocks, "roofline": roof,
             "e2e": {"value": e2e_ev / e2e_s, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "kernel": "batch_kernel (persistent job engine)",
-                         "bytes_per_eval": alg_bytes / max(1, b_ev), "peak_kind": peak_kind,
-                         "traffic": DRAM_BYTES_PER_EVAL["batched"] * b_ev / args.steps},
             # one CUDA graph per step: queue reset, phase-0 seeding, the persistent kernel
-            "gpu_launches": 3 * args.steps}
+            "gpu_launches": 3 * steps}
+
+
+def run_batched(args):
+    import torch
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    import pyhea_b200 as hb
+
+    sub = measure_batched(args.steps, args.warmup, hb.l2_read_probe(L2_PROBE_BYTES))
+    line = {"metric": "swap_evals_per_sec", "n_gpus": 1, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
+    line.update(sub)
     print(json.dumps(line))
     return 0
 
 
-def run_large(args):
-    """FCC 100^3 (4,000,000 sites, 12/6/24 shells, 672 MB neighbour table), 4 species at 0.25,
-    32 solutions x 4096 tasks, depth 20: one iteration per step with every local search capped at
-    --large-rounds rounds.  Occupancies stay in HBM; each solution runs on a thread-block cluster."""
+# ---------------------------------------------------------------------------
+# Large: FCC 100^3
+# ---------------------------------------------------------------------------
+def measure_large(iters, e2e=True):
+    """FCC 100^3 (4,000,000 sites, 12/6/24 shells, 672 MB neighbour table), 4 species at 0.25, 32
+    solutions x 4096 tasks, depth 20: `iters` iterations of the uncapped search (the configuration
+    states 200).  Occupancies stay in HBM; each solution runs on a thread-block cluster."""
+    import numpy as np
     import torch
 
     import pyhea_b200 as hb
     from pyhea_b200 import workloads as W
 
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     st = W.large(seed=0)
     pb = st.problem(device=True)
-    plan = hb.Plan(pb, st.P, 1, st.Q, st.D, max_rounds=args.large_rounds, time_kernels=True)
-    for w in range(args.warmup):
-        plan.run(w)
-    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
-    sampler.start()
-    ms, ev, mc_ms = 0.0, 0, 0.0
-    for k in range(args.steps):  # 4 GB of tables and populations: inputs exceed L2
-        s = plan.run(args.warmup + k)
-        ms += s["gpu_ms"]
-        ev += s["evals"]
-        mc_ms += s["mc_ms"]
+    warm = hb.Plan(pb, st.P, 1, st.Q, st.D, max_rounds=50)  # kernels loaded; capped
+    warm.run(0)
+    warm.close()
+    plan = hb.Plan(pb, st.P, iters, st.Q, st.D, time_kernels=True)
+    sampler = ClockSampler(torch.cuda.current_device()).start()
+    s = plan.run(1)
     clocks = sampler.stop()
     _, fit = plan.read()
     plan.close()
-
-    # end to end through the C ABI with pinned host buffers: the neighbour table uploaded and the
-    # population read back every step (same seeds as the device-timed steps, so the same work)
-    import numpy as np
-
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
-    hp = hb.Problem(pin(pb.nbor), pin(pb.shell_sizes), pin(pb.species), pin(pb.weight), pin(pb.target_sro))
-    out_occ = torch.empty((st.P, st.num_sites), dtype=torch.uint8).pin_memory().numpy()
-    out_fit = torch.empty(st.P, dtype=torch.float64).pin_memory().numpy()
-    e2e_s, e2e_ev = 0.0, 0
-    for k in range(args.steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        _, _, s = hb.search(hp, st.P, 1, st.Q, st.D, seed=args.warmup + k, max_rounds=args.large_rounds,
-                            out_occ=out_occ, out_fitness=out_fit)
-        e2e_s += time.perf_counter() - t0
-        e2e_ev += s["evals"]
-    h2d = hp.nbor.nbytes + hp.shell_sizes.nbytes + hp.species.nbytes + hp.weight.nbytes + hp.target_sro.nbytes
-    d2h = out_occ.nbytes + out_fit.nbytes
-
+    out = {"value": s["evals"] / (s["gpu_ms"] / 1000.0), "unit": "swap-evals/s", "steps": 1, "warmup": 1,
+           "ms_per_step": s["gpu_ms"], "evals_per_step": s["evals"], "rounds_per_step": s["rounds"],
+           "best_fitness": float(fit[0]),
+           "config": {"workload": "large: FCC 100^3, 4,000,000 sites, 12/6/24", "solutions": st.P,
+                      "parallel_task": st.Q, "converge_depth": st.D, "total_iter_run": iters,
+                      "total_iter_stated": st.I, "max_rounds_per_local_search": None,
+                      "warmup": "one capped (50-round) iteration",
+                      "l2": "inputs larger than L2 (704 MB table)"},
+           "clocks": clocks}
     peak, peak_kind = measured_peaks()
     B = st.evals_bytes()
-    achieved = ev * B / (mc_ms / 1000.0) / 1e9
-    line = {"metric": "swap_evals_per_sec", "value": ev / (ms / 1000.0), "unit": "swap-evals/s", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "large: FCC 100^3, 4,000,000 sites, 12/6/24", "solutions": st.P,
-                       "parallel_task": st.Q, "converge_depth": st.D, "total_iter": 1,
-                       "max_rounds_per_local_search": args.large_rounds,
-                       "l2": "inputs larger than L2 (704 MB table)"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "kernel": "mc_large_kernel (cluster local search)", "bytes_per_eval": B,
-                         "peak_kind": peak_kind},
-            "best_fitness_last_step": float(fit[0]), "evals_per_step": ev / args.steps, "clocks": clocks,
-            "e2e": {"value": e2e_ev / e2e_s, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
-            # per step (one iteration): the slot-order reset; zero counts, generate, recount and fitness
-            # for each of the two generations; two cluster local searches; merge and survivor sorts
-            "gpu_launches": args.steps * 13}
+    achieved = s["evals"] * B / (s["mc_ms"] / 1000.0) / 1e9 if s["mc_ms"] > 0 else 0.0
+    out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                       "kernel": "mc_large_kernel (cluster local search)", "bytes_per_eval": B,
+                       "peak_kind": peak_kind, "traffic": None}
+    # per iteration: the slot-order reset; zero counts, generate, recount and fitness for each of the
+    # two generations; two cluster local searches; merge and survivor sorts
+    out["gpu_launches"] = 1 + 12 * iters
+    if e2e:
+        # end to end through the C ABI with pinned host buffers: the neighbour table uploaded and the
+        # population read back (same seed as the device-timed step, so the same work)
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+        hp = hb.Problem(pin(pb.nbor), pin(pb.shell_sizes), pin(pb.species), pin(pb.weight), pin(pb.target_sro))
+        out_occ = torch.empty((st.P, st.num_sites), dtype=torch.uint8).pin_memory().numpy()
+        out_fit = torch.empty(st.P, dtype=torch.float64).pin_memory().numpy()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, _, e = hb.search(hp, st.P, iters, st.Q, st.D, seed=1, out_occ=out_occ, out_fitness=out_fit)
+        dt = time.perf_counter() - t0
+        h2d = hp.nbor.nbytes + hp.shell_sizes.nbytes + hp.species.nbytes + hp.weight.nbytes + hp.target_sro.nbytes
+        out["e2e"] = {"value": e["evals"] / dt, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
+                      "d2h_bytes_per_step": int(out_occ.nbytes + out_fit.nbytes)}
+    return out
+
+
+def run_large(args):
+    import torch
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    line = {"metric": "swap_evals_per_sec", "n_gpus": 1, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
+    line.update(measure_large(args.large_iters))
     print(json.dumps(line))
     return 0
 
 
-def run_serving(args):
-    """Serving loop under a Poisson request stream (workloads.serving): each request an
-    FCC/BCC supercell of 4e3..1e6 sites (log-uniform), 3-6 species, 8 solutions x 256 tasks,
-    4 iterations, depth 10, fitness tolerance 1e-3; tables built on the device from the
-    lattice description.  Requests are submitted at their arrival times while the server
-    runs; latency = arrival to the host holding the result.  value = swap evaluations of
-    the finished requests / wall time of the run."""
-    import math
-
+# ---------------------------------------------------------------------------
+# Serving: a Poisson request stream
+# ---------------------------------------------------------------------------
+def measure_serving(rate, seconds, P, I, slice_ms, warmup=1, Q=256, D=10, tol=1e-3):
+    """Serving loop under a Poisson request stream (workloads.serving): each request an FCC/BCC
+    supercell of 4e3..1e6 sites (log-uniform), 3-6 species, P solutions x Q tasks, up to I
+    iterations, depth D, fitness tolerance `tol`; tables built on the device from the lattice
+    description.  Requests are submitted at their arrival times while the server runs; latency =
+    arrival to the host holding the result.  value = swap evaluations of the finished requests /
+    wall time of the run."""
     import numpy as np
     import torch
 
     import pyhea_b200 as hb
     from pyhea_b200 import workloads as W
 
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    P, Q, I, D, tol = 8, 256, 4, 10, 1e-3
-    reqs = W.serving(seed=0, rate=args.serve_rate, duration=args.serve_seconds, P=P, Q=Q, I=I, D=D)
-    srv = hb.Server(max_requests=1024, arena_bytes=48 << 30, slice_ms=args.slice_ms)
+    reqs = W.serving(seed=0, rate=rate, duration=seconds, P=P, Q=Q, I=I, D=D)
+    srv = hb.Server(max_requests=1024, arena_bytes=48 << 30, slice_ms=slice_ms)
     lo, hi = math.log(4e3), math.log(1e6)
 
     def level(n):  # smaller requests first
@@ -410,7 +490,7 @@ def run_serving(args):
                                   tolerance=tol, priority=level(st.num_sites))
 
     warm = W.serving(seed=1, rate=50.0, duration=1.0, P=P, Q=Q, I=I, D=D)
-    warm = sorted(warm, key=lambda r: r[1].num_sites)[: max(args.warmup, 1)]
+    warm = sorted(warm, key=lambda r: r[1].num_sites)[: max(warmup, 1)]
     for k, (_, st) in enumerate(warm):
         submit(st, 10 ** 6 + k)
     srv.drain()
@@ -419,11 +499,10 @@ def run_serving(args):
     srv.take_finished()
     base = srv.status()
 
-    sampler = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
-    sampler.start()
+    sampler = ClockSampler(torch.cuda.current_device()).start()
     arrival, size, lat, evals, bytes_alg, iters, h2d, d2h = {}, {}, [], 0, 0.0, [], 0, 0
     i, t0 = 0, time.perf_counter()
-    hard_stop = args.serve_seconds + 120.0
+    hard_stop = seconds + 600.0
     last_done = 0.0
     lat_by_size = []  # (sites, latency ms)
     step_gap, step_ms, t_prev = 0.0, 0.0, None  # longest gap between steps; longest step (host view)
@@ -451,8 +530,7 @@ def run_serving(args):
         for rid in srv.take_finished():
             if rid not in arrival:
                 continue
-            r = srv.result(rid)
-            occ, fit, info = r
+            occ, fit, info = srv.result(rid)
             t = time.perf_counter() - t0
             lat.append((t - arrival.pop(rid)) * 1000.0)
             n, B = size.pop(rid)
@@ -479,13 +557,11 @@ def run_serving(args):
     peak, peak_kind = measured_peaks()
     achieved = bytes_alg / (busy / 1000.0) / 1e9 if busy > 0 else 0.0
     value = evals / wall if wall > 0 else 0.0
-    line = {"metric": "swap_evals_per_sec", "value": value, "unit": "swap-evals/s", "n_gpus": 1, "steps": 1,
-            "warmup": len(warm), "ms_per_step": wall * 1000.0, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+    return {"value": value, "unit": "swap-evals/s", "steps": 1, "warmup": len(warm), "ms_per_step": wall * 1000.0,
             "config": {"workload": "serving: Poisson stream of FCC/BCC requests, 4e3..1e6 sites (log-uniform)",
-                       "rate_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds,
-                       "solutions": P, "parallel_task": Q, "total_iter": I, "converge_depth": D, "tolerance": tol,
-                       "slice_ms": args.slice_ms, "priority": "smaller requests first (16 levels by log size)",
+                       "rate_per_s": rate, "arrival_window_s": seconds, "solutions": P, "parallel_task": Q,
+                       "total_iter": I, "converge_depth": D, "tolerance": tol, "slice_ms": slice_ms,
+                       "priority": "smaller requests first (16 levels by log size)",
                        "l2": "inputs larger than L2 (tables of the requests on the device exceed 126 MB)"},
             "requests": {"arrived": i, "finished": len(lat), "unfinished": len(arrival),
                          "per_s": len(lat) / wall if wall > 0 else 0.0,
@@ -502,12 +578,117 @@ def run_serving(args):
                          "frac": achieved / peak, "kernel": "batch_kernel (persistent job engine)",
                          "peak_kind": peak_kind, "traffic": None},
             "gpu_launches": int(st_end["launches"] - base["launches"]), "clocks": clocks}
+
+
+def run_serving(args):
+    import torch
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    line = {"metric": "swap_evals_per_sec", "n_gpus": 1, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
+    line.update(measure_serving(args.serve_rate, args.serve_seconds, args.serve_solutions, args.serve_iters,
+                                args.slice_ms, args.warmup))
     print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# Time to tolerance
+# ---------------------------------------------------------------------------
+def measure_time_to_tol(st, problem, seed, max_iter, tols=(1e-3, 1.02e-3, 1.1e-3, 1.5e-3)):
+    """The structure's search through the serving loop with a fitness tolerance (local searches and
+    the request end once it is reached) and up to max_iter iterations; submission to result on the
+    host.  1e-3 is PyHEA's default threshold (pyhea/model/opt.py:37)."""
+    import pyhea_b200 as hb
+
+    srv = hb.Server(max_requests=4, slice_ms=50.0)
+    q = dict(num_solutions=st.P, total_iter=max_iter, parallel_task=st.Q, converge_depth=st.D, seed=seed)
+    out = []
+    for tol in tols:
+        t0 = time.perf_counter()
+        rid = srv.submit(problem, q, tolerance=tol)
+        res = None
+        while res is None:
+            srv.step()
+            res = srv.result(rid)
+        tt = time.perf_counter() - t0
+        out.append({"tolerance": tol, "wall_ms": 1000.0 * tt, "iterations": res[2]["iterations"],
+                    "best_fitness": float(res[1][0]), "reached": bool(res[1][0] <= tol), "evals": res[2]["evals"]})
+    srv.close()
+    return {"workload": st.name, "solutions": st.P, "parallel_task": st.Q, "converge_depth": st.D,
+            "iteration_cap": max_iter, "result": out[0], "sweep": out}
+
+
+# ---------------------------------------------------------------------------
+# The drop-in module as PyHEA calls it
+# ---------------------------------------------------------------------------
+def measure_dropin(st, nbor, sizes, seed):
+    """accelerate.run_local_parallel_hcs_cuda called positionally as pyhea/model/opt.py:89-90 calls
+    it: neighbour table as nested Python lists [N][S][Z], element counts, weights, target [S][T*T],
+    the per-iteration log line on (the reference prints it); returns lists.  End to end, including
+    the flattening of the nested lists and the Python lists built for the result.  The library
+    prints the log lines on file descriptor 1; they are counted here, not passed on."""
+    import pyhea_b200 as hb
+    from pyhea_b200 import lattice as L
+
+    nested = L.as_nested(nbor, sizes)
+    species = [int(x) for x in st.species]
+    weight = [float(w) for w in st.weight]
+    sys.stdout.flush()
+    saved = os.dup(1)
+    with tempfile.TemporaryFile() as log:
+        os.dup2(log.fileno(), 1)
+        try:
+            t0 = time.perf_counter()
+            latts, fits = hb.accelerate.run_local_parallel_hcs_cuda(st.P, st.I, st.Q, st.D, 0.001, nested, species,
+                                                                    weight, st.target, seed=seed)
+            dt = time.perf_counter() - t0
+        finally:
+            os.dup2(saved, 1)
+            os.close(saved)
+        log.seek(0)
+        lines = log.read().decode(errors="replace").count("best fitness")
+    return {"wall_ms": dt * 1000.0, "logged_lines": lines, "best_fitness": float(fits[0]),
+            "note": "value = the plain search's evaluations per step over this call's wall time"}
+
+
+def run_case(args):
+    """One small fixed case for profiler captures; prints its statistics as JSON."""
+    import numpy as np
+
+    import pyhea_b200 as hb
+    from pyhea_b200 import lattice as L
+    from pyhea_b200 import workloads as W
+
+    if args.case == "plain":
+        st = W.plain_gpu(seed=0)
+        plan = hb.Plan(st.problem(device=True), st.P, args.iters, st.Q, st.D)
+        out = plan.run(123)
+        plan.close()
+    elif args.case == "batch":
+        structs = sorted(W.batched(seed=0), key=lambda s: -s.num_sites)[: args.count]
+        problems = [st.problem(device=True) for st in structs]
+        params = [dict(num_solutions=st.P, total_iter=args.iters, parallel_task=st.Q, converge_depth=st.D)
+                  for st in structs]
+        b = hb.Batch(problems, params)
+        out = b.run([11 + i for i in range(len(structs))])
+        b.close()
+    else:
+        rng = np.random.default_rng(0)
+        n = 4 * args.cell ** 3
+        st = W.Structure(L.FCC, args.cell, L.SHELLS_FCC_TRUE3, [n // 4] * 4, W.WEIGHTS,
+                         W.zero_row_sum_target(rng, 4, 0.05), P=32, Q=4096, I=1, D=20, name=f"fcc{args.cell}")
+        plan = hb.Plan(st.problem(device=True), st.P, 1, st.Q, st.D, max_rounds=args.rounds, hbm_occupancy=True)
+        out = plan.run(123)
+        plan.close()
+    print(json.dumps(out))
     return 0
 
 
 def main():
     args = parse_args()
+    if args.case:
+        return run_case(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batched":
@@ -531,13 +712,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
 
     import pyhea_b200 as hb
+    from pyhea_b200 import replicas
 
+    l2_peak = hb.l2_read_probe(L2_PROBE_BYTES)
     st = workload(args.workload)
     problem = st.problem(device=True)
     nbor, sizes = st.neighbors(device=True)
     plan = hb.Plan(problem, st.P, st.I, st.Q, st.D, time_kernels=True, autotune=True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    from pyhea_b200 import replicas
 
     for w in range(args.warmup):
         plan.run(replicas.replica_seed(rank, w))
@@ -545,8 +727,7 @@ def main():
     if dist:
         dist.barrier()
 
-    sampler = ClockSampler(local)
-    sampler.start()
+    sampler = ClockSampler(local).start()
     total_ms, evals, mc_ms, launches, accepts = 0.0, 0, 0.0, 0, 0
     for k in range(args.steps):
         flush.zero_()
@@ -581,67 +762,53 @@ def main():
     h2d = (hp.nbor.nbytes + hp.shell_sizes.nbytes + hp.species.nbytes + hp.weight.nbytes + hp.target_sro.nbytes)
     d2h = out_occ.nbytes + out_fit.nbytes
 
-    # time to tolerance: the same search through the serving loop with a fitness tolerance (local
-    # searches and the request end once it is reached), submission to result on the host; 1e-3 is
-    # PyHEA's default threshold, the looser ones show the time along the way
-    time_to_tol = None
-    time_to_tol_sweep = []
-    if rank == 0:
-        srv = hb.Server(max_requests=4, slice_ms=50.0)
-        q = dict(num_solutions=st.P, total_iter=st.I, parallel_task=st.Q, converge_depth=st.D,
-                 seed=replicas.replica_seed(rank, 20_000))
-        for tol in (1e-3, 1.02e-3, 1.1e-3, 1.5e-3):
-            t0 = time.perf_counter()
-            rid = srv.submit(problem, q, tolerance=tol)
-            res = None
-            while res is None:
-                srv.step()
-                res = srv.result(rid)
-            tt = time.perf_counter() - t0
-            time_to_tol_sweep.append({"tolerance": tol, "wall_ms": 1000.0 * tt, "iterations": res[2]["iterations"],
-                                      "best_fitness": float(res[1][0]), "reached": bool(res[1][0] <= tol),
-                                      "evals": res[2]["evals"]})
-        srv.close()
-        time_to_tol = time_to_tol_sweep[0]
-
     dev = torch.device("cuda", local)
     total_ms_max, evals_all = replicas.combine(total_ms, evals, device=dev)
     e2e_ms_max, e2e_evals_all = replicas.combine(1000.0 * e2e_s, e2e_evals, device=dev)
     e2e_max = e2e_ms_max / 1000.0
 
     if rank == 0:
-        peak, peak_kind = measured_peaks()
         B = st.evals_bytes()
-        achieved = evals * B / (mc_ms / 1000.0) / 1e9 if mc_ms > 0 else None
+        counters = KERNEL_COUNTERS.get(args.workload, {"dram": None, "capture": None})
+        roof = roofline_of("mc_kernel (local search)", counters, evals, mc_ms / 1000.0, B, launches, clocks, l2_peak,
+                           sm_count())
+        roof["kernel_share"] = mc_ms / total_ms if total_ms else None
         line = {
             "metric": "swap_evals_per_sec", "value": evals_all / (total_ms_max / 1000.0), "unit": "swap-evals/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(config_of(st, args.workload), parallelism=f"replicas x{world}",
                            local_search_block=block),
-            "gpu_launches": None,
+            # kernels launched per search: 1 generate + per iteration (generate, search, merge, search,
+            # sort), plus the iota of the slot order
+            "gpu_launches": args.steps * (2 + 5 * st.I),
             "e2e": {"value": e2e_evals_all / e2e_max, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None,
-                         "traffic": (DRAM_BYTES_PER_EVAL[args.workload] * evals / launches
-                                     if args.workload in DRAM_BYTES_PER_EVAL and launches else None),
-                         "algorithmic_bytes_per_launch": evals * B / launches if launches else None,
-                         "kernel": "mc_kernel (local search)", "bytes_per_eval": B, "peak_kind": peak_kind,
-                         "kernel_share": mc_ms / total_ms if total_ms else None},
+            "roofline": roof,
             "search": {"evals_per_step": evals / args.steps, "accepts_per_step": accepts / args.steps,
                        "best_fitness_last_step": float(best[0])},
-            "time_to_tol": time_to_tol, "time_to_tol_sweep": time_to_tol_sweep,
             "clocks": clocks,
         }
-        # kernels launched per search: 1 generate + per iteration (generate, search, merge, search, sort), plus
-        # the iota of the slot order
-        line["gpu_launches"] = args.steps * (2 + 5 * st.I)
-        if world == 1 and not args.no_cpu_baseline:
-            r = cpu_reference_sample(st, nbor, sizes, args.cpu_procs or host_cores())
-            if r:
-                line["cpu_baseline"] = {"value": r["evals"] / r["wall_s"], "unit": "swap-evals/s", "cores": r["procs"],
-                                        "kind": "reference", "sample": r["sample"]}
+        if world == 1:
+            d = measure_dropin(st, nbor, sizes, replicas.replica_seed(rank, 30_000))
+            d["value"] = (evals / args.steps) / (d["wall_ms"] / 1000.0)
+            d["unit"] = "swap-evals/s"
+            line["dropin_e2e"] = d
+            line["time_to_tol"] = measure_time_to_tol(st, problem, replicas.replica_seed(rank, 20_000),
+                                                      args.tol_iters)
+            if not args.no_extras:
+                cpu = workload("plain_cpu")
+                line["time_to_tol_plain_cpu"] = measure_time_to_tol(cpu, cpu.problem(device=True), 20_000,
+                                                                    args.tol_iters)
+                line["batched"] = measure_batched(args.steps, args.warmup, l2_peak)
+                line["serving"] = measure_serving(args.serve_rate, args.serve_seconds, args.serve_solutions,
+                                                  args.serve_iters, args.slice_ms)
+                line["large"] = measure_large(args.large_iters)
+            if not args.no_cpu_baseline:
+                r = cpu_reference_sample(st, nbor, sizes, args.cpu_procs or host_cores())
+                if r:
+                    line["cpu_baseline"] = {"value": r["evals"] / r["wall_s"], "unit": "swap-evals/s",
+                                            "cores": r["procs"], "kind": "reference", "sample": r["sample"]}
         print(json.dumps(line))
     if dist:
         dist.barrier()

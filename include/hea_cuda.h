@@ -88,6 +88,14 @@ const char *hea_last_error(void);
  * cached buffers to the driver.  No counterpart in the reference. */
 void hea_release_cached_memory(void);
 
+/* L2 read bandwidth of the current device, the denominator of the search
+ * kernels' L2 roofline (their tables and site histograms stay in L2 at the
+ * benchmark sizes): every SM reads a buffer of `bytes` (it must fit in L2;
+ * 16-byte loads through L2 only) `reps` times after one warm-up pass; *out_gbs
+ * = bytes * reps / CUDA-event time.  A measurement aid with no counterpart in
+ * the reference. */
+int hea_l2_read_probe(int64_t bytes, int32_t reps, double *out_gbs);
+
 /*
  * The whole search, host buffers in and out: replaces
  * accelerate::gpu::run_local_parallel_hcs_cuda (accelerate.cu:1112-1242).
@@ -138,6 +146,12 @@ int hea_batch_tallies(hea_batch *batch, uint64_t *out);
  * kernel's resident CTAs per SM or one fewer, and keeps the fastest.  Results
  * do not depend on the choice.  Outputs may be NULL. */
 int hea_batch_autotune(hea_batch *batch, int32_t *out_hbm_all, int32_t *out_ctas_per_sm);
+/* Bound on every wait of the persistent kernel for queued work (default 60 s):
+ * a CTA that finds no job for this long after the last finished one sets the
+ * batch's error flag and every CTA returns; hea_batch_run then fails with a
+ * message and the next run starts clean.  No counterpart in the reference
+ * (its kernels never wait on one another). */
+int hea_batch_set_wait_limit(hea_batch *batch, double ms);
 void hea_batch_destroy(hea_batch *batch);
 
 /*
@@ -174,6 +188,8 @@ typedef struct hea_server_config {
     int32_t hbm_sites;     /* occupancy in HBM for structures of at least this many sites; 0: all (the
                               default, fastest with histogram scoring); -1: only those beyond smem_bytes */
     double slice_ms;       /* length of one step's launch (0: 20 ms)                             */
+    double wait_limit_ms;  /* bound on every wait inside the kernel for queued work (0: 10 s); a CTA
+                              whose wait runs out stops the slice with an error and the server stops */
 } hea_server_config;
 
 typedef struct hea_request_info {

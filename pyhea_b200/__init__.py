@@ -73,7 +73,7 @@ class AcceptRecord(ctypes.Structure):
 
 class _ServerConfig(ctypes.Structure):
     _fields_ = [("max_requests", _i32), ("ring_jobs", _i32), ("arena_bytes", _i64), ("smem_bytes", _i32),
-                ("hbm_sites", _i32), ("slice_ms", _f64)]
+                ("hbm_sites", _i32), ("slice_ms", _f64), ("wait_limit_ms", _f64)]
 
 
 class RequestInfo(ctypes.Structure):
@@ -110,6 +110,7 @@ def _declare(lib):
         "hea_local_search": (_i32, [_P(_Problem), _u64, _u32, _i32, _i32, _i32, _i64, _P(_u8), _P(_i32), _P(_f64),
                                     _P(_i64), _P(AcceptRecord), _P(_i32), _i64, _P(_i64)]),
         "hea_build_neighbors": (_i32, [_i32, _i32, _i32, _P(_i32), _P(_i32), _P(_i32)]),
+        "hea_l2_read_probe": (_i32, [_i64, _i32, _P(_f64)]),
         "hea_recount_noalloc": (_i32, [_P(_Problem), _i32, _P(_u8), _P(_i32), _P(_f64)]),
         "hea_batch_create": (_i32, [_P(_Problem), _P(_Params), _i32, _P(ctypes.c_void_p)]),
         "hea_batch_run": (_i32, [ctypes.c_void_p, _P(_u64), _P(Stats)]),
@@ -117,6 +118,7 @@ def _declare(lib):
         "hea_batch_finish_times": (_i32, [ctypes.c_void_p, _P(_f64)]),
         "hea_batch_tallies": (_i32, [ctypes.c_void_p, _P(_u64)]),
         "hea_batch_autotune": (_i32, [ctypes.c_void_p, _P(_i32), _P(_i32)]),
+        "hea_batch_set_wait_limit": (_i32, [ctypes.c_void_p, _f64]),
         "hea_batch_destroy": (None, [ctypes.c_void_p]),
         "hea_server_create": (_i32, [_P(_ServerConfig), _P(ctypes.c_void_p)]),
         "hea_server_submit": (_i32, [ctypes.c_void_p, _P(_Problem), _P(_Params), _f64, _i32, _P(_i64)]),
@@ -296,6 +298,11 @@ class Batch:
         _check(_load().hea_batch_autotune(self._h, ctypes.byref(h), ctypes.byref(c)))
         return {"hbm_all": h.value, "ctas_per_sm": c.value}
 
+    def set_wait_limit(self, ms):
+        """Bound (ms) on every wait of the persistent kernel for queued work; a run whose wait runs
+        out raises HeaError and leaves the batch ready for the next run."""
+        _check(_load().hea_batch_set_wait_limit(self._h, float(ms)))
+
     def finish_times(self):
         """Milliseconds from the start of the last run to each structure's end."""
         out = np.empty(len(self.problems))
@@ -331,9 +338,10 @@ class Server:
     result equals search() on it alone with the same seed (with a tolerance:
     with total_iter = info["iterations"])."""
 
-    def __init__(self, max_requests=0, ring_jobs=0, arena_bytes=0, smem_bytes=0, slice_ms=0.0, hbm_sites=0):
+    def __init__(self, max_requests=0, ring_jobs=0, arena_bytes=0, smem_bytes=0, slice_ms=0.0, hbm_sites=0,
+                 wait_limit_ms=0.0):
         cfg = _ServerConfig(int(max_requests), int(ring_jobs), int(arena_bytes), int(smem_bytes), int(hbm_sites),
-                            float(slice_ms))
+                            float(slice_ms), float(wait_limit_ms))
         self._h = ctypes.c_void_p()
         _check(_load().hea_server_create(ctypes.byref(cfg), ctypes.byref(self._h)))
         self._meta = {}  # id -> (P, N)
@@ -506,3 +514,11 @@ def build_neighbors(lattice, cell, shell_set=SHELLS_REFERENCE):
     _check(_load().hea_build_neighbors(int(lattice), int(cell), int(shell_set), _ptr(nbor, _i32), _ptr(sizes, _i32),
                                    ctypes.byref(n)))
     return nbor, sizes
+
+
+def l2_read_probe(nbytes=32 << 20, reps=50):
+    """hea_l2_read_probe: L2 read bandwidth of the current device in GB/s (a buffer of
+    `nbytes` that fits in L2, read `reps` times by every SM)."""
+    out = _f64()
+    _check(_load().hea_l2_read_probe(int(nbytes), int(reps), ctypes.byref(out)))
+    return out.value

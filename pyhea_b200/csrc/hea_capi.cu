@@ -674,10 +674,19 @@ struct hea_plan {
     std::vector<cudaEvent_t> mc_events;  // start/stop pairs, HEA_FLAG_TIME_KERNELS
     int mc_timed = 0;
     int mc_block = 0;  // threads per CTA of the local search (choose_block, or the autotuner's pick)
+    // HEA_FLAG_LOG_ITERS: each iteration's best f2 written by the device into mapped pinned memory
+    // and printed by a host callback on the stream (no host synchronisation per iteration)
+    struct LogEntry {
+        int it;
+        const double *best;
+    };
+    double *log_host = nullptr, *log_dev = nullptr;
+    std::vector<LogEntry> log_entries;
     ~hea_plan()
     {
         if (stream) cudaStreamSynchronize(stream);  // buffers return to the pool only when idle
         if (side) cudaStreamSynchronize(side);
+        if (log_host) cudaFreeHost(log_host);
         for (cudaEvent_t e : mc_events) cudaEventDestroy(e);
         for (cudaEvent_t e : joins) cudaEventDestroy(e);
         if (side) cudaStreamDestroy(side);
@@ -818,6 +827,34 @@ void log_iteration(int it, double best)
     std::fflush(stdout);
 }
 
+// The best f2 of a sorted population (slot order[0]) into *out (mapped pinned memory).
+__global__ void best_f2_kernel(const int32_t *order, const double *f2, double *out) { *out = f2[order[0]]; }
+
+// Stream host callback: prints the log line of one iteration once the device
+// has written its best f2 (no CUDA calls here).
+void CUDART_CB log_callback(void *arg)
+{
+    const hea_plan::LogEntry *e = static_cast<const hea_plan::LogEntry *>(arg);
+    log_iteration(e->it, std::sqrt(*e->best));
+}
+
+// Mapped pinned memory for one best f2 per iteration (HEA_FLAG_LOG_ITERS).
+int plan_log_buffers(hea_plan *pl)
+{
+    const int I = pl->prm.total_iter;
+    if (!(pl->prm.flags & HEA_FLAG_LOG_ITERS) || I < 1 || (int)pl->log_entries.size() >= I) return HEA_OK;
+    if (pl->log_host) {
+        HEA_CUDA(cudaStreamSynchronize(pl->stream));
+        cudaFreeHost(pl->log_host);
+        pl->log_host = nullptr;
+    }
+    HEA_CUDA(cudaHostAlloc((void **)&pl->log_host, sizeof(double) * I, cudaHostAllocMapped));
+    HEA_CUDA(cudaHostGetDevicePointer((void **)&pl->log_dev, pl->log_host, 0));
+    pl->log_entries.resize(I);
+    for (int it = 0; it < I; ++it) pl->log_entries[it] = hea_plan::LogEntry{it, pl->log_host + it};
+    return HEA_OK;
+}
+
 int read_population(hea_plan *pl, int count, uint8_t *out_occ, double *out_fitness)
 {
     const SearchConst &c = pl->dt.c;
@@ -849,6 +886,7 @@ int plan_search(hea_plan *pl, hea_stats *stats)
             pl->mc_events.push_back(e);
         }
     }
+    HEA_TRY(plan_log_buffers(pl));
     HEA_CUDA(cudaMemsetAsync(pl->stats, 0, 4 * sizeof(unsigned long long), pl->stream));
     iota_kernel<<<(2 * P + 255) / 256, 256, 0, pl->stream>>>(pl->order, 2 * P);
     HEA_CUDA(cudaGetLastError());
@@ -873,14 +911,10 @@ int plan_search(hea_plan *pl, hea_stats *stats)
         }
         HEA_TRY(launch_mc(pl, pl->order, P, (uint32_t)(2 * it + 1), McArgs{}));
         HEA_TRY(launch_sort(pl, pl->order, P));
-        if (pl->prm.flags & HEA_FLAG_LOG_ITERS) {
-            int32_t best_slot = 0;
-            double best = 0;
-            HEA_CUDA(cudaMemcpyAsync(&best_slot, pl->order, sizeof(int32_t), cudaMemcpyDeviceToHost, pl->stream));
-            HEA_CUDA(cudaStreamSynchronize(pl->stream));
-            HEA_CUDA(cudaMemcpyAsync(&best, pl->f2 + best_slot, sizeof(double), cudaMemcpyDeviceToHost, pl->stream));
-            HEA_CUDA(cudaStreamSynchronize(pl->stream));
-            log_iteration(it, std::sqrt(best));
+        if (pl->prm.flags & HEA_FLAG_LOG_ITERS) {  // the reference's per-iteration line (accelerate.cu:1208-1212)
+            best_f2_kernel<<<1, 1, 0, pl->stream>>>(pl->order, pl->f2, pl->log_dev + it);
+            HEA_CUDA(cudaGetLastError());
+            HEA_CUDA(cudaLaunchHostFunc(pl->stream, log_callback, &pl->log_entries[it]));
         }
         if (it + 1 < I) {
             HEA_CUDA(cudaStreamWaitEvent(pl->stream, pl->joins[1], 0));
@@ -1075,6 +1109,61 @@ int hea_cuda_available(void)
 }
 
 const char *hea_last_error(void) { return g_error.c_str(); }
+
+}  // extern "C"
+
+namespace {
+// Reads the buffer `reps` times with 16-byte loads through L2 (four in flight
+// per thread); the xor of everything read goes to *sink only if it matches a
+// value it never takes in practice, so the loads are not removed.
+__global__ void __launch_bounds__(256) l2_read_probe_kernel(const uint4 *buf, int64_t n16, int reps, uint32_t *sink)
+{
+    uint32_t acc = 0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int r = 0; r < reps; ++r)
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n16; i += 4 * stride) {
+            uint4 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) v[u] = i + u * stride < n16 ? __ldcg(buf + i + u * stride) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc ^= v[u].x ^ v[u].y ^ v[u].z ^ v[u].w;
+        }
+    if (acc == 0x9E3779B9u) atomicAdd(sink, 1u);
+}
+}  // namespace
+
+extern "C" {
+
+int hea_l2_read_probe(int64_t bytes, int32_t reps, double *out_gbs)
+{
+    if (bytes < (1 << 20) || reps < 1 || !out_gbs) return fail(HEA_ERR_INVALID, "bytes >= 1 MiB, reps >= 1, out_gbs");
+    int dev = 0, sms = 0, l2 = 0;
+    HEA_CUDA(cudaGetDevice(&dev));
+    HEA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    HEA_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+    if (bytes > l2) return fail(HEA_ERR_INVALID, "%lld bytes do not fit in the %d-byte L2", (long long)bytes, l2);
+    const int64_t n16 = bytes / 16;
+    DeviceBuf buf, sink;
+    HEA_CUDA(dev_alloc(&buf.p, (size_t)n16 * 16));
+    HEA_CUDA(dev_alloc(&sink.p, sizeof(uint32_t)));
+    HEA_CUDA(cudaMemset(buf.p, 1, (size_t)n16 * 16));
+    cudaEvent_t e0, e1;
+    HEA_CUDA(cudaEventCreate(&e0));
+    HEA_CUDA(cudaEventCreate(&e1));
+    const int grid = sms * 8;
+    l2_read_probe_kernel<<<grid, 256>>>((const uint4 *)buf.p, n16, 1, (uint32_t *)sink.p);  // brings it into L2
+    cudaEventRecord(e0);
+    l2_read_probe_kernel<<<grid, 256>>>((const uint4 *)buf.p, n16, reps, (uint32_t *)sink.p);
+    cudaEventRecord(e1);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail(HEA_ERR_CUDA, "L2 probe failed: %s", cudaGetErrorString(e));
+    *out_gbs = (double)n16 * 16.0 * reps / (ms * 1e-3) / 1e9;
+    return HEA_OK;
+}
 
 int hea_plan_create(const hea_problem *problem, const hea_params *params, hea_plan **out)
 {
@@ -1462,6 +1551,7 @@ struct hea_batch {
     double *out_f2 = nullptr;
     BatchLevels_ *lv = nullptr;  // queue layout of the graph's reset kernel
     int hbm_all = 1, ctas_per_sm = HEA_BATCH_MIN_BLOCKS;  // current launch configuration
+    unsigned long long wait_limit_ns = 60ull * 1000000000ull;  // bound on every device-side wait
     ~hea_batch()
     {
         delete lv;
@@ -1580,7 +1670,7 @@ int batch_configure(hea_batch *b, int hbm_all, int ctas_per_sm)
     b->graph = nullptr;
     // the run as one CUDA graph: reset the queue, seed phase 0, persistent kernel
     HEA_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    batch_reset_kernel<<<64, 256, 0, b->stream>>>(b->d_ctl, b->d_jobs, b->total_jobs, *b->lv, 60ull * 1000000000ull);
+    batch_reset_kernel<<<64, 256, 0, b->stream>>>(b->d_ctl, b->d_jobs, b->total_jobs, *b->lv, b->wait_limit_ns);
     batch_seed_kernel<<<b->count, 256, 0, b->stream>>>(b->d_structs, nullptr, b->d_states, b->d_jobs, b->d_ctl);
     batch_kernel<<<b->grid, b->block, b->smem, b->stream>>>(b->d_structs, b->d_states, b->d_jobs, b->d_ctl,
                                                             b->d_finish);
@@ -1728,6 +1818,14 @@ int hea_batch_run(hea_batch *b, const uint64_t *seeds, hea_stats *stats)
         stats->mc_launches = 1;
     }
     return HEA_OK;
+}
+
+int hea_batch_set_wait_limit(hea_batch *b, double ms)
+{
+    if (!b) return fail(HEA_ERR_INVALID, "batch is NULL");
+    if (!(ms > 0.0) || ms > 3.6e6) return fail(HEA_ERR_INVALID, "wait limit must be in (0, 3600000] ms");
+    b->wait_limit_ns = (unsigned long long)(ms * 1e6);
+    return batch_configure(b, b->hbm_all, b->ctas_per_sm);  // the limit is a parameter of the captured reset
 }
 
 int hea_batch_autotune(hea_batch *b, int32_t *out_hbm_all, int32_t *out_ctas_per_sm)
@@ -2318,6 +2416,8 @@ int hea_server_create(const hea_server_config *config, hea_server **out)
     if (cfg.max_requests <= 0) cfg.max_requests = 256;
     if (cfg.ring_jobs <= 0) cfg.ring_jobs = 65536;
     if (cfg.slice_ms <= 0) cfg.slice_ms = 20.0;
+    if (cfg.wait_limit_ms <= 0) cfg.wait_limit_ms = 10000.0;
+    if (cfg.wait_limit_ms > 3.6e6) return fail(HEA_ERR_INVALID, "wait_limit_ms must be <= 3600000");
     if (cfg.max_requests > 65536) return fail(HEA_ERR_INVALID, "max_requests must be <= 65536");
     if (cfg.ring_jobs > (1 << 26)) return fail(HEA_ERR_INVALID, "ring_jobs must be <= 2^26");
     hea_server *sv = new (std::nothrow) hea_server();
@@ -2386,7 +2486,7 @@ int hea_server_create(const hea_server_config *config, hea_server **out)
             }
             batch_reset_kernel<<<64, 256, 0, sv->stream>>>(sv->d_ctl, sv->d_jobs,
                                                           (unsigned long long)cfg.ring_jobs * kBatchLevels, lv,
-                                                          10ull * 1000000000ull);
+                                                          (unsigned long long)(cfg.wait_limit_ms * 1e6));
             e = cudaGetLastError();
         }
         if (e == cudaSuccess) e = cudaStreamSynchronize(sv->stream);

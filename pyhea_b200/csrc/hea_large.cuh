@@ -227,9 +227,12 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
             const auto after = [cold, &w, a, b](int k, int i, int j) {
                 return cold[(k * T + i) * T + j] + count_change<T>(w, a, b, k, i, j);
             };
-            for (int x = tid; x < NC; x += blockDim.x) cnew[x] = after(x / (T * T), (x / T) % T, x % T);
+            const int me = block_rotation(32 * accept_linear_warps<T, S>());
+            for (int x = me; x < NC; x += blockDim.x) cnew[x] = after(x / (T * T), (x / T) % T, x % T);
             delta_linear<T, S>(c, tab, after);
-            if (rank == 0) update_hist<L, true>(c, g.nbor, hist, w.s1, w.s2, a, b);
+            if (rank == 0)
+                update_hist<L, true>(c, g.nbor, hist, w.s1, w.s2, a, b,
+                                     block_rotation(32 * (accept_linear_warps<T, S>() + (NC + 31) / 32)));
             cluster.sync();  // the cluster's next proposals read the updated histograms; each CTA its table
             buf ^= 1;
             cur = __dadd_rn(cur, key_delta(xk));

@@ -268,14 +268,16 @@ __device__ __forceinline__ double score_delta(const SearchConst &c, const int4 *
 // kSpeciesWord: also the species words of s1 and s2, which draw_pair_hist
 // reads; searches whose draws read the occupancy leave them at their recount
 // values.
+// `me` is this thread's index in the block's order of the work (a rotation of
+// threadIdx.x, so that other updates can run on the first warps meanwhile).
 template <class L, bool kSpeciesWord>
 __device__ __forceinline__ void update_hist(const SearchConst &c, const int4 *__restrict__ nbor, uint4 *hist,
-                                            uint32_t s1, uint32_t s2, int a, int b)
+                                            uint32_t s1, uint32_t s2, int a, int b, int me)
 {
     const int row4 = L::kRuntime ? c.row4 : L::kRow4;
     const int row = 4 * row4;
     const uint32_t up = (1u << (5 * b)) - (1u << (5 * a));  // s1's neighbours: one a becomes b
-    for (int e = threadIdx.x; e < 2 * row; e += blockDim.x) {
+    for (int e = me; e < 2 * row; e += blockDim.x) {
         const bool first = e < row;
         const int idx = first ? e : e - row;
         const int32_t *r = reinterpret_cast<const int32_t *>(nbor + (size_t)(first ? s1 : s2) * row4);
@@ -287,10 +289,23 @@ __device__ __forceinline__ void update_hist(const SearchConst &c, const int4 *__
         uint32_t *h = reinterpret_cast<uint32_t *>(hist + n) + k;
         atomicAdd(h, first ? up : 0u - up);
     }
-    if (kSpeciesWord && threadIdx.x == 0) {
+    if (kSpeciesWord && me == 0) {
         hist[s1].w = (uint32_t)(5 * b);
         hist[s2].w = (uint32_t)(5 * a);
     }
+}
+
+// The three updates of an accepted swap on different warps where the block has
+// enough of them: the table's L half on warps [0, delta_linear's warps), the
+// new counts on the next warps, the neighbours' histograms after those.  The
+// rotated thread indices (block_rotation) keep every loop covering its work once.
+template <int T, int S>
+__host__ __device__ constexpr int accept_linear_warps() { return (S * T + 32 / T - 1) / (32 / T); }
+__device__ __forceinline__ int block_rotation(int by)
+{
+    int me = (int)threadIdx.x - by;
+    while (me < 0) me += blockDim.x;
+    return me;
 }
 
 // Two attempts per Philox call: (x0, x1) then (x2, x3); valid when both draws
@@ -685,9 +700,11 @@ __device__ __forceinline__ McTally mc_rounds(const SearchConst &c, const int4 *_
             const auto after = [cold, &w, a, b](int k, int i, int j) {
                 return cold[(k * T + i) * T + j] + count_change<T>(w, a, b, k, i, j);
             };
-            for (int x = tid; x < NC; x += blockDim.x) cnew[x] = after(x / (T * T), (x / T) % T, x % T);
+            const int me = block_rotation(32 * accept_linear_warps<T, S>());
+            for (int x = me; x < NC; x += blockDim.x) cnew[x] = after(x / (T * T), (x / T) % T, x % T);
             delta_linear<T, S>(c, tab, after);
-            update_hist<L, false>(c, nbor, hist, w.s1, w.s2, a, b);
+            update_hist<L, false>(c, nbor, hist, w.s1, w.s2, a, b,
+                                  block_rotation(32 * (accept_linear_warps<T, S>() + (NC + 31) / 32)));
             const double D = key_delta(xk);
             __syncthreads();  // next round's proposals read the new table and histograms
             buf ^= 1;

@@ -10,6 +10,19 @@ It also restates the per-shell alpha of a set of pair counts with the
 reference's formula alpha_ij = 1 - gamma_ij / (c_i c_j), gamma = C / (Z_k N)
 (pyhea/cpp/accelerate.cpp:171), so a searched structure can be compared to its
 target without the third-party analyzer.
+
+And it restates the analyzer the reference runs on its output files
+(pyhea/utils/analyze.py:12-45): OVITO's WarrenCowleyParameters modifier with
+nneigh = [0, 12, 18] (FCC) or [0, 8, 14] (BCC), the third-party package
+WarrenCowleyParameters >= 2.0.0 (pyhea requirements.txt:10; not installed
+here, so this restatement is unpinned against it).  Its published definition
+(Cowley, Phys. Rev. 77, 669 (1950)): for each atom the neighbours are ranked
+by distance (periodic images), shell m holds ranks nneigh[m] .. nneigh[m+1]-1,
+and alpha^m_ij = 1 - P^m(j | i) / c_j, where P^m(j | i) is the fraction of
+species-j atoms among the shell-m neighbours of species-i atoms and c_j the
+concentration of j.  warren_cowley() computes that from positions and types;
+where the rank ranges are whole coordination shells (FCC 12 + 6, BCC 8 + 6)
+it equals alpha_from_counts on the engine's first two shells.
 """
 import os
 
@@ -92,3 +105,50 @@ def weighted_sro_error(counts, shell_sizes, species, weight, target):
     t = np.asarray(target, dtype=np.float64).reshape(a.shape)
     w = np.asarray(weight, dtype=np.float64)
     return float(np.sqrt(np.sum(w * np.sum((a - t) ** 2, axis=(1, 2)))))
+
+
+ANALYZER_NNEIGH = {"FCC": (0, 12, 18), "BCC": (0, 8, 14)}  # pyhea/utils/analyze.py:35
+
+
+def warren_cowley(positions, box, types, num_types=None, nneigh=(0, 12, 18)):
+    """Warren-Cowley parameters [len(nneigh)-1][T][T] of a periodic structure, by neighbour rank.
+
+    positions [N][3] Cartesian, box [3] edge lengths of an orthogonal periodic cell, types [N] in
+    [0, T).  For every atom its nneigh[-1] nearest other atoms (minimum image) are ranked by
+    distance; shell m is ranks [nneigh[m], nneigh[m+1]).  alpha^m_ij = 1 - P^m(j|i) / c_j with
+    P^m(j|i) = (species-j neighbours in shell m of species-i atoms) / (n_i * shell size).
+    A rank range that splits a set of equidistant neighbours depends on their order; keep the
+    ranges at whole coordination shells."""
+    from scipy.spatial import cKDTree
+
+    pos = np.asarray(positions, dtype=np.float64)
+    box = np.asarray(box, dtype=np.float64)
+    types = np.asarray(types, dtype=np.int64)
+    T = int(num_types) if num_types is not None else int(types.max()) + 1
+    edges = [int(x) for x in nneigh]
+    if edges[0] != 0 or any(b <= a for a, b in zip(edges, edges[1:])):
+        raise ValueError("nneigh must start at 0 and increase")
+    tree = cKDTree(np.mod(pos, box), boxsize=box)
+    _, idx = tree.query(np.mod(pos, box), k=edges[-1] + 1)
+    nb = idx[:, 1:]  # rank 0 is the atom itself
+    counts = np.bincount(types, minlength=T).astype(np.float64)
+    c = counts / counts.sum()
+    out = np.zeros((len(edges) - 1, T, T))
+    for m in range(len(edges) - 1):
+        ranks = nb[:, edges[m]:edges[m + 1]]
+        pair = np.zeros((T, T))
+        np.add.at(pair, (np.repeat(types, ranks.shape[1]), types[ranks].ravel()), 1.0)
+        P = pair / (counts[:, None] * ranks.shape[1])
+        out[m] = 1.0 - P / c[None, :]
+    return out
+
+
+def warren_cowley_of_occupancy(occupancy, lattice, cell, num_types=None, nneigh=None):
+    """warren_cowley() of an occupancy on the FCC (0) / BCC (1) cube of edge `cell` in the
+    engine's site numbering, with the reference analyzer's rank ranges by default."""
+    from . import lattice as _lat
+
+    if nneigh is None:
+        nneigh = ANALYZER_NNEIGH["FCC" if lattice == _lat.FCC else "BCC"]
+    pos = _lat.positions(lattice, cell).astype(np.float64) * 0.5  # lattice units
+    return warren_cowley(pos, np.full(3, float(cell)), occupancy, num_types, nneigh)

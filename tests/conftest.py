@@ -36,3 +36,17 @@ def engine_case_problem(case, golden_nbor, module):
     ss = case["shell_size"]
     nbor = golden_nbor[lat][:, : int(ss.sum())]
     return module.Problem(nbor, ss, case["species"], case["weight"], case["target"])
+
+
+def opt_call_args():
+    """The positional arguments the reference driver passes to run_local_parallel_hcs_cuda
+    (pyhea/model/opt.py:89-90), rebuilt with the recorded types (tests/golden/opt_call.json,
+    made by tests/golden/make_golden.py opt)."""
+    import json
+
+    d = json.load(open(os.path.join(GOLDEN, "opt_call.json")))
+    a = list(d["args"])
+    assert d["arg_types"][5] == "list[list[ndarray(int64)]]" and d["arg_types"][8] == "ndarray(float64)"
+    a[5] = [[np.asarray(shell, dtype=np.int64) for shell in site] for site in a[5]]
+    a[8] = np.asarray(a[8], dtype=np.float64)
+    return a

@@ -18,6 +18,12 @@ Fixtures written:
                      (pyhea/io/output.py:62-106) for seeded occupancies of FCC and
                      BCC cells (`python tests/golden/make_golden.py poscar` writes
                      only these)
+  opt_call.json      the positional call the reference's own driver makes into its engine
+                     (pyhea/model/opt.py:87-90, device: gpu), recorded by running
+                     opt_model.run_optimization on an FCC 4^3 configuration read by the
+                     reference config reader, with a recording stand-in in place of
+                     pyhea.cpp.accelerate (`python tests/golden/make_golden.py opt` writes
+                     only this)
   lammps_conf.json   the reference's sample LAMMPS output (examples/conf.lmp, FCC
                      10^3, 4 species): its occupancy in the reference lattice's site
                      order, its lattice constant and the SHA-256 of its text
@@ -96,7 +102,88 @@ def lammps_fixture(lattice):
         json.dump(fixture, f, indent=1)
 
 
+def opt_call_fixture():
+    """Run the reference's opt_model.run_optimization (device: gpu) with a stand-in engine module
+    that records the positional arguments of run_local_parallel_hcs_cuda and returns a valid
+    population, so the driver completes (and writes its POSCAR) as it would with a real engine."""
+    import types
+
+    calls = []
+
+    def run_cuda(*args):
+        calls.append(args)
+        nnet, element = args[0], args[6]
+        occ = [t for t, c in enumerate(element) for _ in range(c)]
+        rng = np.random.default_rng(0)
+        latts = [[int(x) for x in rng.permutation(occ)] for _ in range(nnet)]
+        return latts, [0.1 * (i + 1) for i in range(nnet)]
+
+    fake = types.ModuleType("pyhea.cpp.accelerate")
+    fake.run_local_parallel_hcs_cuda = run_cuda
+    fake.cuda_available = lambda: True
+    fake.run_local_parallel_hcs = None
+    sys.modules["pyhea.cpp.accelerate"] = fake
+    lattice, input_config = import_reference()
+    import pyhea.cpp  # noqa: E402  (package of the stand-in)
+
+    pyhea.cpp.accelerate = fake
+    import pyhea.io.input as reference_input  # noqa: E402
+    from pyhea.model.opt import opt_model  # noqa: E402
+
+    # the config reader falls back to device: cpu unless it sees a GPU; this machine has none
+    reference_input.get_gpu_info = lambda: [{"name": "NVIDIA B200", "memory": "183359 MiB", "driver": "580"}]
+
+    class OneRank:  # mpi4py.MPI.COMM_WORLD of a single process
+        def Get_rank(self):
+            return 0
+
+        def Get_size(self):
+            return 1
+
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        cfg = os.path.join(tmp, "config.yaml")
+        with open(cfg, "w") as f:
+            f.write("type: 4\nelement: [64, 64, 64, 64]\ncell_dim: [4, 4, 4]\ndevice: gpu\nsolutions: 4\n"
+                    "total_iter: 2\nparallel_task: 32\nconverge_depth: 4\nweight: [4.0, 1.0, 0.5]\n"
+                    f"structure: {os.path.join(REFERENCE_ROOT, 'examples', 'POSCAR_FCC')}\n"
+                    f"target_sro: {os.path.join(REFERENCE_ROOT, 'examples', 'TARGET_SRO')}\n")
+        conf = input_config(cfg)
+        latt = lattice(conf.cell_dim, conf.latt_type, conf.latt_const, conf.latt_vectors, valid=True)
+        os.chdir(tmp)
+        try:
+            opt_model(latt, conf, OneRank()).run_optimization()
+            written = sorted(os.listdir(tmp))
+        finally:
+            os.chdir(cwd)
+    assert len(calls) == 1
+    args = calls[0]
+    def kind(a):  # type of an argument down to its innermost containers, e.g. "list[list[ndarray(int64)]]"
+        if isinstance(a, np.ndarray):
+            return f"ndarray({a.dtype})"
+        if isinstance(a, (list, tuple)):
+            return f"{type(a).__name__}[{kind(a[0])}]" if len(a) else f"{type(a).__name__}[]"
+        return type(a).__name__
+
+    def plain(a):
+        if isinstance(a, np.ndarray):
+            return a.tolist()
+        if isinstance(a, (list, tuple)):
+            return [plain(x) for x in a]
+        return a.item() if isinstance(a, np.generic) else a
+
+    kinds = [kind(a) for a in args]
+    as_json = [plain(a) for a in args]
+    with open(os.path.join(HERE, "opt_call.json"), "w") as f:
+        json.dump({"source": "pyhea/model/opt.py:87-90 (device: gpu), FCC 4^3 from examples/POSCAR_FCC, "
+                             "target from examples/TARGET_SRO", "arg_types": kinds, "args": as_json,
+                   "files_written": written}, f)
+
+
 def main():
+    if sys.argv[1:] == ["opt"]:
+        opt_call_fixture()
+        return
     lattice, input_config = import_reference()
     if sys.argv[1:] == ["poscar"]:
         poscar_fixtures(lattice)
@@ -106,6 +193,7 @@ def main():
         return
     poscar_fixtures(lattice)
     lammps_fixture(lattice)
+    opt_call_fixture()
 
     # 1. neighbour lists
     nb = {}

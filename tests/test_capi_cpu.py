@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import pyhea_b200 as hb
-from conftest import REPO
+from conftest import REPO, opt_call_args
 from pyhea_b200 import accelerate
 from pyhea_b200 import lattice as L
 
@@ -83,3 +83,14 @@ def test_pybind_argument_errors():
         accelerate.run_local_parallel_hcs_cuda(2, 1, 8, 2, 0.001, bad, [27] * 4, [4.0, 1.0, 0.5], tgt)
     with pytest.raises(RuntimeError, match="CPU engine"):
         accelerate.run_local_parallel_hcs(2, 1, 8, 2, 0.001, nested, [27] * 4, [4.0, 1.0, 0.5], tgt)
+
+
+@pytest.mark.skipif(hb.cuda_available(), reason="checks argument handling on a machine without a GPU")
+def test_reference_driver_call_is_accepted():
+    """The exact positional call of the reference driver (recorded from pyhea/model/opt.py:89-90:
+    neighbour shells as numpy arrays in nested lists, target as an ndarray) is parsed by the
+    drop-in module, which fails only at the device step here."""
+    args = opt_call_args()
+    with pytest.raises(RuntimeError) as err:
+        accelerate.run_local_parallel_hcs_cuda(*args)
+    assert not isinstance(err.value, (TypeError, ValueError))

@@ -11,10 +11,11 @@ import os
 import numpy as np
 import pytest
 
-from conftest import REPO, engine_case_problem
+from conftest import REPO, engine_case_problem, opt_call_args
 from oracle import hea_oracle as ho
 import pyhea_b200 as hb
 from pyhea_b200 import lattice as L
+from pyhea_b200 import sro
 from pyhea_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
@@ -160,6 +161,30 @@ def test_dropin_module_call_as_pyhea_model_makes_it():
     np.testing.assert_array_equal(np.array(fitss), np.sqrt(wf2))
 
 
+def test_dropin_replays_the_reference_driver_call(capfd):
+    """The call recorded from the reference driver (pyhea/model/opt.py:89-90, device: gpu) through
+    the drop-in module: with a seed it equals the oracle's search; as recorded (no keywords: fresh
+    seed, log on) it returns a valid population and prints one log line per iteration."""
+    args = opt_call_args()
+    nnet, step, task, depth, thr, nbor, element, weight, target = args
+    nb = np.array([np.concatenate(site) for site in nbor], dtype=np.int32)
+    sizes = np.array([len(s) for s in nbor[0]], dtype=np.int32)
+    op = ho.Problem(nb, sizes, element, weight, target)
+    latts, fitss = hb.accelerate.run_local_parallel_hcs_cuda(*args, seed=2024, verbose=False)
+    wocc, wf2, _ = op.hcs(2024, nnet, step, task, depth)
+    np.testing.assert_array_equal(np.array(latts), wocc)
+    np.testing.assert_array_equal(np.array(fitss), np.sqrt(wf2))
+    capfd.readouterr()
+    latts, fitss = hb.accelerate.run_local_parallel_hcs_cuda(*args)
+    out = capfd.readouterr().out
+    assert out.count("best fitness") == step
+    assert len(latts) == nnet and fitss == sorted(fitss)
+    for o, f in zip(latts, fitss):
+        o = np.array(o, dtype=np.uint8)
+        np.testing.assert_array_equal(np.bincount(o, minlength=len(element)), element)
+        assert f == np.sqrt(op.f2(op.recount(o)))
+
+
 def test_search_fitness_agrees_with_reference_engine():
     """Final structures scored by the reference's calculate_fitness_of_solutions."""
     path = os.path.join(REPO, "oracle", "_ref", "libref_accelerate.so")
@@ -274,3 +299,19 @@ def test_autotuned_plan_gives_the_same_search():
         np.testing.assert_array_equal(ref.read()[1], tuned.read()[1])
     ref.close()
     tuned.close()
+
+
+@pytest.mark.parametrize("case", [CASES[0], CASES[6], CASES[7]])
+def test_searched_alpha_in_the_analyzer_convention(case):
+    """Final alpha of searched structures: alpha from the device's pair counts (the engine's
+    convention) equals the analyzer-convention restatement (neighbour ranks [0, 12, 18] FCC /
+    [0, 8, 14] BCC, pyhea/utils/analyze.py:35) computed from the occupancies, shells 1-2."""
+    lat, cell = case[0], case[1]
+    gp, _ = pair(case)
+    occ, fit, _ = hb.search(gp, 4, 2, 64, 4, seed=3)
+    cnt, f2 = hb.recount(gp, occ)
+    np.testing.assert_array_equal(np.sqrt(f2), fit)
+    for p in range(len(occ)):
+        a = sro.alpha_from_counts(cnt[p], gp.shell_sizes, gp.species)
+        wc = sro.warren_cowley_of_occupancy(occ[p], lat, cell, gp.num_types)
+        np.testing.assert_allclose(wc, a[:2], rtol=0, atol=1e-12)

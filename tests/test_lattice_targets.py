@@ -103,3 +103,39 @@ def test_alpha_matches_reference_gamma(golden_engine, golden_nbor):
             gamma = np.moveaxis(np.asarray(case["gamma"][p]), -1, 0)  # [T][T][S] -> [S][T][T]
             ref_alpha = 1.0 - gamma / np.outer(c, c)[None]
             np.testing.assert_allclose(a, ref_alpha, rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("lat,cell,T", [(L.FCC, 5, 4), (L.BCC, 6, 3), (L.FCC, 4, 6), (L.BCC, 10, 5)])
+def test_analyzer_restatement_equals_alpha_from_counts(lat, cell, T):
+    """The analyzer's convention (pyhea/utils/analyze.py:35: neighbour ranks [0, 12, 18] FCC,
+    [0, 8, 14] BCC) gives, on perfect lattices, the engine-convention alpha of shells 1-2."""
+    from oracle import hea_oracle as ho
+
+    nbor, sizes = L.neighbors(lat, cell)
+    n = L.num_sites(lat, cell)
+    for seed in range(3):
+        occ = np.random.default_rng(seed).permutation(np.arange(n) % T).astype(np.uint8)
+        sp = np.bincount(occ, minlength=T)
+        op = ho.Problem(nbor, sizes, sp, [4.0, 1.0, 0.5], np.zeros((3, T * T)))
+        wc = sro.warren_cowley_of_occupancy(occ, lat, cell, T)
+        a = sro.alpha_from_counts(op.recount(occ), sizes, sp)
+        assert wc.shape == (2, T, T)
+        np.testing.assert_allclose(wc, a[:2], rtol=0, atol=1e-12)
+        np.testing.assert_allclose(wc, wc.transpose(0, 2, 1), rtol=0, atol=1e-12)
+
+
+def test_analyzer_restatement_on_a_written_structure_file(tmp_path):
+    """End to end as the reference post-processes (write the structure, analyse the file): a POSCAR
+    written by the reference-format writer and read back gives the same parameters."""
+    from pyhea_b200 import output
+
+    lat, cell, T = L.FCC, 4, 4
+    n = L.num_sites(lat, cell)
+    occ = np.random.default_rng(7).permutation(np.arange(n) % T)
+    path = str(tmp_path / "out.poscar")
+    output.write_poscar(path, occ, lat, cell, lattice_constant=3.6, num_types=T)
+    scale, vec, labels, counts, coords = output.read_poscar(path)
+    types = np.repeat(np.arange(T), counts)
+    got = sro.warren_cowley(coords * scale, np.diag(vec) * scale, types, T, sro.ANALYZER_NNEIGH["FCC"])
+    want = sro.warren_cowley_of_occupancy(occ, lat, cell, T)
+    np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
