@@ -5,6 +5,10 @@ Produces
   oracle/_ref/libref_accelerate.so the reference CPU engine, compiled from the
                                    reference's own pyhea/cpp/accelerate.cpp with
                                    ref_harness.cpp and the single-rank MPI stub
+  oracle/_ref/pymod/accelerate<ext> the reference's own pybind11 module (its
+                                   pyhea/cpp/bind.cpp + accelerate.cpp, CPU engine
+                                   only), for the test of the install layout that
+                                   keeps `device: cpu` beside the drop-in
 
 The reference tree is read in place from REFERENCE_ROOT: the environment
 variable HEA_REFERENCE_ROOT, else a checkout named `reference` beside this
@@ -57,8 +61,31 @@ def build_reference():
     return out
 
 
+def build_reference_module():
+    """PyHEA's own `accelerate` extension module as its build makes it for the CPU engine
+    (bind.cpp + accelerate.cpp, no USE_CUDA), with the single-rank MPI stub."""
+    import sysconfig
+
+    src_dir = os.path.join(REFERENCE_ROOT, "pyhea", "cpp")
+    if not os.path.exists(os.path.join(src_dir, "bind.cpp")):
+        return None
+    out_dir = os.path.join(HERE, "_ref", "pymod")
+    os.makedirs(out_dir, exist_ok=True)
+    out = os.path.join(out_dir, "accelerate" + sysconfig.get_config_var("EXT_SUFFIX"))
+    srcs = [os.path.join(src_dir, "bind.cpp"), os.path.join(src_dir, "accelerate.cpp")]
+    deps = srcs + [os.path.join(HERE, "mpi_stub", "mpi.h")]
+    if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps):
+        return out
+    import pybind11
+
+    _run(["g++", "-O3", "-std=c++14", "-fPIC", "-shared", "-include", "tuple", "-I", os.path.join(HERE, "mpi_stub"),
+          "-I", src_dir, "-I", sysconfig.get_paths()["include"], "-I", pybind11.get_include(), *srcs, "-o", out])
+    return out
+
+
 if __name__ == "__main__":
     print(build_oracle())
+    print(build_reference_module() or "reference tree not found; oracle/_ref/pymod left as is")
     r = build_reference()
     print(r if r else "reference tree not found; oracle/_ref left as is")
     sys.exit(0)
