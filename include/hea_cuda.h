@@ -96,6 +96,13 @@ void hea_release_cached_memory(void);
  * the reference. */
 int hea_l2_read_probe(int64_t bytes, int32_t reps, double *out_gbs);
 
+/* Random 16-byte loads per second from a buffer of `bytes` (far larger than
+ * L2), each through L2 only, per_thread loads by each of 8 CTAs x 256 threads
+ * per SM after one warm-up launch: the ceiling of the site-histogram loads of
+ * structures whose histograms stay in DRAM (each load moves a 32-byte sector).
+ * A measurement aid with no counterpart in the reference. */
+int hea_dram_random_probe(int64_t bytes, int32_t per_thread, double *out_loads_per_s);
+
 /*
  * The whole search, host buffers in and out: replaces
  * accelerate::gpu::run_local_parallel_hcs_cuda (accelerate.cu:1112-1242).

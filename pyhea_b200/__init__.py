@@ -111,6 +111,7 @@ def _declare(lib):
                                     _P(_i64), _P(AcceptRecord), _P(_i32), _i64, _P(_i64)]),
         "hea_build_neighbors": (_i32, [_i32, _i32, _i32, _P(_i32), _P(_i32), _P(_i32)]),
         "hea_l2_read_probe": (_i32, [_i64, _i32, _P(_f64)]),
+        "hea_dram_random_probe": (_i32, [_i64, _i32, _P(_f64)]),
         "hea_recount_noalloc": (_i32, [_P(_Problem), _i32, _P(_u8), _P(_i32), _P(_f64)]),
         "hea_batch_create": (_i32, [_P(_Problem), _P(_Params), _i32, _P(ctypes.c_void_p)]),
         "hea_batch_run": (_i32, [ctypes.c_void_p, _P(_u64), _P(Stats)]),
@@ -521,4 +522,11 @@ def l2_read_probe(nbytes=32 << 20, reps=50):
     `nbytes` that fits in L2, read `reps` times by every SM)."""
     out = _f64()
     _check(_load().hea_l2_read_probe(int(nbytes), int(reps), ctypes.byref(out)))
+    return out.value
+
+
+def dram_random_probe(nbytes=4 << 30, per_thread=256):
+    """hea_dram_random_probe: random 16-byte loads per second from a buffer of `nbytes` in DRAM."""
+    out = _f64()
+    _check(_load().hea_dram_random_probe(int(nbytes), int(per_thread), ctypes.byref(out)))
     return out.value

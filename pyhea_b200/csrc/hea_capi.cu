@@ -1130,9 +1130,66 @@ __global__ void __launch_bounds__(256) l2_read_probe_kernel(const uint4 *buf, in
         }
     if (acc == 0x9E3779B9u) atomicAdd(sink, 1u);
 }
+
+// Random 16-byte loads through L2 from a buffer far larger than L2, eight in
+// flight per thread: the access pattern of the site-histogram loads of
+// structures whose histograms do not fit in L2.  Indices come from the murmur3
+// finaliser of a per-thread counter, mapped to [0, n16) by a multiply-high.
+__global__ void __launch_bounds__(256) dram_random_probe_kernel(const uint4 *buf, uint64_t n16, int per_thread,
+                                                                uint32_t seed, uint32_t *sink)
+{
+    uint32_t acc = 0;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int i = 0; i < per_thread; i += 8) {
+        uint4 v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const uint32_t h = fmix32(seed ^ (t * 0x9E3779B9u) ^ (uint32_t)(i + u) * 0x85EBCA6Bu);
+            const uint64_t idx = ((uint64_t)h * n16) >> 32;
+            v[u] = __ldcg(buf + idx);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc ^= v[u].x ^ v[u].w;
+    }
+    if (acc == 0x9E3779B9u) atomicAdd(sink, 1u);
+}
 }  // namespace
 
 extern "C" {
+
+int hea_dram_random_probe(int64_t bytes, int32_t per_thread, double *out_loads_per_s)
+{
+    if (bytes < ((int64_t)1 << 28) || per_thread < 8 || per_thread % 8 || !out_loads_per_s)
+        return fail(HEA_ERR_INVALID, "bytes >= 256 MiB, per_thread a positive multiple of 8, out_loads_per_s");
+    int dev = 0, sms = 0;
+    HEA_CUDA(cudaGetDevice(&dev));
+    HEA_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const uint64_t n16 = (uint64_t)bytes / 16;
+    if (n16 > 0xFFFFFFFFull) return fail(HEA_ERR_INVALID, "at most 64 GiB");
+    struct Owned {  // the probe's buffer goes back to the driver, not to the block cache
+        void *p = nullptr;
+        ~Owned() { if (p) cudaFree(p); }
+    } buf, sink;
+    if (cudaMalloc(&buf.p, (size_t)n16 * 16) != cudaSuccess || cudaMalloc(&sink.p, sizeof(uint32_t)) != cudaSuccess)
+        return fail(HEA_ERR_NOMEM, "cannot allocate %lld bytes for the probe", (long long)bytes);
+    HEA_CUDA(cudaMemset(buf.p, 1, (size_t)n16 * 16));
+    cudaEvent_t e0, e1;
+    HEA_CUDA(cudaEventCreate(&e0));
+    HEA_CUDA(cudaEventCreate(&e1));
+    const int grid = sms * 8;
+    dram_random_probe_kernel<<<grid, 256>>>((const uint4 *)buf.p, n16, 8, 1u, (uint32_t *)sink.p);
+    cudaEventRecord(e0);
+    dram_random_probe_kernel<<<grid, 256>>>((const uint4 *)buf.p, n16, per_thread, 7u, (uint32_t *)sink.p);
+    cudaEventRecord(e1);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail(HEA_ERR_CUDA, "DRAM probe failed: %s", cudaGetErrorString(e));
+    *out_loads_per_s = (double)grid * 256.0 * per_thread / (ms * 1e-3);
+    return HEA_OK;
+}
 
 int hea_l2_read_probe(int64_t bytes, int32_t reps, double *out_gbs)
 {
