@@ -74,15 +74,22 @@ HBM_FALLBACK_GBS = 6650.0
 #   dram   dram__bytes_read.sum + dram__bytes_write.sum      -> roofline.traffic
 #   l2     lts__t_sectors_srcunit_tex.sum x 32 B              -> roofline.l2_frac
 #   inst   smsp__inst_executed.sum (warp instructions)        -> roofline.issue_frac
+#   dram_read  dram__bytes_read.sum                           -> roofline.dram_random (batched)
 # mc_kernel<5, Shells<2,2,3>>: the first local-search launch of `python bench.py --case plain
-# --iters 1` (203.72 M evaluations): 163.78 MB DRAM, 433.1 M L2 sectors, 3.808 G warp instructions.
-# batch_kernel: one launch of `python bench.py --case batch --count 64 --iters 1`.
+# --iters 1` (203.72 M evaluations): 71.68 MB + 93.46 MB DRAM, 437.14 M L2 sectors, 3.9646 G warp
+# instructions.  batch_kernel: the launch of `python bench.py --case batch --count 64 --iters 1`
+# (631.34 M evaluations): 131.64 GB + 9.28 GB DRAM, 8.890 G L2 sectors, 21.76 G warp instructions.
+# dram_random_probe_kernel (hea_dram_random_probe over 4 GiB, 77.59 M random 16-byte loads):
+# 9.833 GB DRAM read, i.e. 126.7 B per load (each random load fetches a 128-byte line).
 KERNEL_COUNTERS = {
-    "plain_gpu": {"dram": 163.78e6 / 203.72e6, "l2": 2.126 * 32.0, "inst": 18.69,
+    "plain_gpu": {"dram": (71.68e6 + 93.46e6) / 203.72e6, "l2": 437.14e6 * 32.0 / 203.72e6,
+                  "inst": 3.9646e9 / 203.72e6,
                   "capture": "mc_kernel, first local-search launch of bench.py --case plain --iters 1"},
-    "batched": {"dram": 152.467e9 / 631.335e6, "l2": None, "inst": None,
+    "batched": {"dram": (131.64e9 + 9.28e9) / 631.34e6, "l2": 8.890e9 * 32.0 / 631.34e6, "inst": 21.76e9 / 631.34e6,
+                "dram_read": 131.64e9 / 631.34e6,
                 "capture": "batch_kernel, bench.py --case batch --count 64 --iters 1"},
 }
+DRAM_BYTES_PER_RANDOM_LOAD = 9.833e9 / 77.594624e6
 L2_PROBE_BYTES = 32 << 20  # fits in L2 (126 MB) with room to spare
 
 
@@ -374,6 +381,16 @@ def measure_batched(steps, warmup, l2_peak=None):
     bpe = sum(e * st.evals_bytes() for e, st in zip(evals_of, structs)) / max(1, sum(evals_of))
     roof = roofline_of("batch_kernel (persistent job engine)", KERNEL_COUNTERS["batched"], b_ev, b_ms / 1000.0,
                        bpe, steps, clocks, l2_peak, sm_count())
+    # the ceiling that binds the batch: most of its evaluations are on structures whose site
+    # histograms stay in DRAM, read at random; random 16-byte DRAM loads are measured here by the
+    # library's probe and converted to DRAM bytes with the probe's captured bytes per load
+    loads_per_s = hb.dram_random_probe(4 << 30, 256)
+    peak_dram = loads_per_s * DRAM_BYTES_PER_RANDOM_LOAD / 1e9
+    got_dram = value * KERNEL_COUNTERS["batched"]["dram_read"] / 1e9
+    roof["dram_random"] = {"probe_loads_per_s": loads_per_s, "dram_bytes_per_probe_load": DRAM_BYTES_PER_RANDOM_LOAD,
+                           "peak_gbs": peak_dram, "dram_read_bytes_per_eval": KERNEL_COUNTERS["batched"]["dram_read"],
+                           "achieved_gbs": got_dram, "unit": "GB/s"}
+    roof["dram_random_frac"] = got_dram / peak_dram
     return {"value": value, "unit": "swap-evals/s", "steps": steps, "warmup": warmup, "ms_per_step": b_ms / steps,
             "config": {"workload": "batched: 64 mixed FCC/BCC structures",
                        "sites_total": int(sum(st.num_sites for st in structs)), "solutions": 64,
