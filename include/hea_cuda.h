@@ -48,6 +48,17 @@ typedef struct hea_problem {
     const int32_t *species;      /* [T] atoms of each species ("element")             */
     const double *weight;        /* [S] shell weights                                 */
     const double *target_sro;    /* [S][T*T] target Warren-Cowley alpha, row-major    */
+    /* Optional implicit neighbours (no counterpart in the reference, which
+     * always passes a table, lattice.py:196-323): with nbor == NULL, a perfect
+     * FCC/BCC cube described here stands for the table, its neighbour ids are
+     * computed on the device from lattice arithmetic and no table is stored.
+     * implicit_lattice: 1 FCC, 2 BCC (0: none, nbor required); lattice_cell:
+     * the cube's edge in unit cells (N = 4 or 2 cell^3); lattice_shell_set as in
+     * hea_build_neighbors.  shell_sizes must be the lattice's for the first S
+     * shells.  Results equal those with the table hea_build_neighbors builds. */
+    int32_t implicit_lattice;
+    int32_t lattice_cell;
+    int32_t lattice_shell_set;
 } hea_problem;
 
 /* Search controls: nnet, step, task, depth, thr of the reference call

@@ -50,7 +50,8 @@ class HeaValueError(HeaError, ValueError):
 
 class _Problem(ctypes.Structure):
     _fields_ = [("num_sites", _i32), ("num_types", _i32), ("num_shells", _i32), ("shell_sizes", _P(_i32)),
-                ("nbor", _P(_i32)), ("species", _P(_i32)), ("weight", _P(_f64)), ("target_sro", _P(_f64))]
+                ("nbor", _P(_i32)), ("species", _P(_i32)), ("weight", _P(_f64)), ("target_sro", _P(_f64)),
+                ("implicit_lattice", _i32), ("lattice_cell", _i32), ("lattice_shell_set", _i32)]
 
 
 class _Params(ctypes.Structure):
@@ -180,21 +181,39 @@ def _ptr(a, ct):
 class Problem:
     """One structure: flattened neighbour table [N][sum Z], shell sizes, species
     counts, shell weights and target alpha [S][T*T] (the reference's nbor,
-    element, weight and target_sro with nbor cut to len(weight) shells)."""
+    element, weight and target_sro with nbor cut to len(weight) shells).
 
-    def __init__(self, nbor, shell_sizes, species, weight, target_sro):
+    ``Problem.from_lattice`` describes a perfect FCC/BCC cube instead of giving a
+    table: the device computes neighbour ids from lattice arithmetic and stores
+    no table (same results as with the table ``build_neighbors`` makes)."""
+
+    def __init__(self, nbor, shell_sizes, species, weight, target_sro, lattice=None):
         self.species = np.ascontiguousarray(species, dtype=np.int32)
         self.weight = np.ascontiguousarray(weight, dtype=np.float64)
         S, T = len(self.weight), len(self.species)
         sizes = np.asarray(shell_sizes, dtype=np.int32)
         self.shell_sizes = np.ascontiguousarray(sizes[:S])
-        nb = np.asarray(nbor)
-        self.nbor = np.ascontiguousarray(nb[:, : int(self.shell_sizes.sum())], dtype=np.int32)
+        if nbor is None:
+            self.nbor = None
+        else:
+            nb = np.asarray(nbor)
+            self.nbor = np.ascontiguousarray(nb[:, : int(self.shell_sizes.sum())], dtype=np.int32)
         self.target_sro = np.ascontiguousarray(np.asarray(target_sro, dtype=np.float64).reshape(-1, T * T)[:S])
         self.num_sites = int(self.species.sum())
         self.num_types, self.num_shells = T, S
+        self.lattice = lattice  # (FCC | BCC, cell, shell_set) of an implicit-neighbour problem, else None
+        kind, cell, shell_set = (lattice[0] + 1, lattice[1], lattice[2]) if lattice is not None else (0, 0, 0)
         self._c = _Problem(self.num_sites, T, S, _ptr(self.shell_sizes, _i32), _ptr(self.nbor, _i32),
-                           _ptr(self.species, _i32), _ptr(self.weight, _f64), _ptr(self.target_sro, _f64))
+                           _ptr(self.species, _i32), _ptr(self.weight, _f64), _ptr(self.target_sro, _f64),
+                           int(kind), int(cell), int(shell_set))
+
+    @classmethod
+    def from_lattice(cls, lattice, cell, species, weight, target_sro, shell_set=SHELLS_REFERENCE):
+        """Implicit-neighbour problem of the FCC (0) / BCC (1) cube of edge `cell`."""
+        from . import lattice as _lat
+
+        sizes = [len(v) for v in _lat.shell_vectors(lattice, shell_set)]
+        return cls(None, sizes, species, weight, target_sro, lattice=(int(lattice), int(cell), int(shell_set)))
 
     @property
     def ncount(self):

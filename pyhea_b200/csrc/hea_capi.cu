@@ -301,6 +301,21 @@ __global__ void nbmask_kernel(const int32_t *padded, int num_sites, int pad_row,
 
 size_t nbmask_words(int num_sites) { return ((size_t)2 * num_sites - 1 + 31) / 32; }
 
+// The same bitmap for implicit neighbours: `row` computed neighbours per site.
+__global__ void nbmask_implicit_kernel(const SearchConst c, int row, uint32_t *mask)
+{
+    const int64_t total = (int64_t)c.num_sites * row;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
+        const int s = (int)(x / row), e = (int)(x % row);
+        const int n = lattice_neighbor(c.lat, site_pos(c.lat, s), e);
+        const uint32_t d = (uint32_t)(n - s + c.num_sites - 1);
+        atomicOr(mask + (d >> 5), 1u << (d & 31u));
+    }
+}
+
+// Neighbours per site the implicit rows hold for the first S shells.
+int implicit_row(const SearchConst &c, int S) { return c.lat.zoff[S - 1] + c.lat.zsize[S - 1]; }
+
 __global__ void gather_rows_kernel(const uint8_t *occ, const int32_t *order, int count, int stride, int n,
                                    const double *f2, uint8_t *out, double *out_f2)
 {
@@ -458,7 +473,8 @@ int validate_problem(const hea_problem *pb, bool need_nbor = true)
     if (pb->num_shells < 1 || pb->num_shells > kMaxShells)
         return fail(HEA_ERR_UNSUPPORTED, "number of shells (len(weight)) must be 1..%d, got %d", kMaxShells,
                     pb->num_shells);
-    if (!pb->shell_sizes || (need_nbor && !pb->nbor) || !pb->species || !pb->weight || !pb->target_sro)
+    const bool implicit = !pb->nbor && pb->implicit_lattice != 0;
+    if (!pb->shell_sizes || (need_nbor && !pb->nbor && !implicit) || !pb->species || !pb->weight || !pb->target_sro)
         return fail(HEA_ERR_INVALID, "problem has a NULL array");
     int64_t n = 0;
     for (int t = 0; t < pb->num_types; ++t) {
@@ -481,7 +497,48 @@ int validate_problem(const hea_problem *pb, bool need_nbor = true)
             if (!std::isfinite(pb->target_sro[(size_t)k * pb->num_types * pb->num_types + x]))
                 return fail(HEA_ERR_INVALID, "target_sro[%d][%d] is not finite", k, x);
     }
+    if (implicit) {  // the lattice stands for the table: it must describe this structure
+        if (pb->implicit_lattice < 1 || pb->implicit_lattice > 2)
+            return fail(HEA_ERR_INVALID, "implicit_lattice must be 1 (FCC) or 2 (BCC), got %d", pb->implicit_lattice);
+        if (pb->lattice_shell_set < 0 || pb->lattice_shell_set > 1)
+            return fail(HEA_ERR_INVALID, "lattice_shell_set must be 0 or 1, got %d", pb->lattice_shell_set);
+        const int64_t L = pb->lattice_cell, nb = pb->implicit_lattice == 1 ? 4 : 2;
+        if (L < 2 || L > 1024 || nb * L * L * L != n)
+            return fail(HEA_ERR_INVALID, "a %s cube of edge %lld does not hold %lld sites",
+                        pb->implicit_lattice == 1 ? "FCC" : "BCC", (long long)L, (long long)n);
+        LatticeSpec sp;
+        HEA_TRY(make_lattice_spec(pb->implicit_lattice - 1, pb->lattice_shell_set, sp));
+        for (int k = 0; k < pb->num_shells; ++k)
+            if (pb->shell_sizes[k] != sp.size[k])
+                return fail(HEA_ERR_INVALID, "shell %d of that lattice has %d neighbours, shell_sizes says %d", k,
+                            sp.size[k], pb->shell_sizes[k]);
+    }
     return HEA_OK;
+}
+
+// Lattice descriptor of an implicit-neighbour problem (validated), or L = 0.
+void fill_lattice_const(const hea_problem *pb, SearchConst &c)
+{
+    std::memset(&c.lat, 0, sizeof(c.lat));
+    if (pb->nbor || pb->implicit_lattice == 0) return;
+    LatticeSpec sp;
+    make_lattice_spec(pb->implicit_lattice - 1, pb->lattice_shell_set, sp);
+    LatticeConst &lc = c.lat;
+    lc.L = pb->lattice_cell;
+    lc.nb = sp.nb;
+    int e = 0;
+    for (int k = 0; k < 3; ++k) {
+        lc.zoff[k] = e;
+        lc.zsize[k] = sp.size[k];
+        for (int v = 0; v < sp.size[k]; ++v, ++e)
+            for (int d = 0; d < 3; ++d) lc.vec[e][d] = (int8_t)sp.vec[k][v][d];
+    }
+    for (int b = 0; b < 4; ++b)
+        for (int d = 0; d < 3; ++d) lc.basis[b][d] = (int8_t)(b < sp.nb ? sp.basis[b][d] : 0);
+    for (int q = 0; q < 8; ++q) lc.lut[q] = -1;
+    for (int b = 0; b < sp.nb; ++b)
+        lc.lut[((sp.basis[b][0] & 1) << 2) | ((sp.basis[b][1] & 1) << 1) | (sp.basis[b][2] & 1)] = (int8_t)b;
+    for (int k = 0; k < kMaxShells; ++k) c.pad[k] = 0;  // no sentinel padding in computed rows
 }
 
 int validate_params(const hea_params *pr)
@@ -577,6 +634,7 @@ void fill_const(const hea_problem *pb, uint64_t seed, SearchConst &c, PadGeom &g
                 c.R[e] = (double)N / (((double)pb->shell_sizes[k] * (double)pb->species[i]) * (double)pb->species[j]);
             }
     }
+    fill_lattice_const(pb, c);
 }
 
 int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t flags = 0)
@@ -609,6 +667,17 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t
         dt.mc = pick_mc(T, c.chunks[0], S > 1 ? c.chunks[1] : 0, S > 2 ? c.chunks[2] : 0, S);
         HEA_CUDA(allow_max_smem(dt.gen));
         HEA_CUDA(allow_max_smem(dt.mc));
+    }
+
+    if (c.lat.L) {  // implicit neighbours: no table, the bitmap from lattice arithmetic
+        const size_t words = nbmask_words(N);
+        if (dev_alloc(&dt.nbmask, words * sizeof(uint32_t)) != cudaSuccess)
+            return fail(HEA_ERR_NOMEM, "cannot allocate the neighbour-offset bitmap");
+        HEA_CUDA(cudaMemset(dt.nbmask, 0, words * sizeof(uint32_t)));
+        nbmask_implicit_kernel<<<1184, 256>>>(c, implicit_row(c, S), dt.nbmask);
+        HEA_CUDA(cudaGetLastError());
+        HEA_CUDA(cudaStreamSynchronize(0));
+        return HEA_OK;
     }
 
     // padded table on the device, checked
@@ -1455,6 +1524,8 @@ extern "C" int hea_recount_noalloc(const hea_problem *problem, int32_t count, co
 {
     if (count < 1 || count > 65535) return fail(HEA_ERR_INVALID, "count must be 1..65535");
     if (!occ) return fail(HEA_ERR_INVALID, "occ is NULL");
+    if (problem && !problem->nbor)
+        return fail(HEA_ERR_UNSUPPORTED, "the allocation-free recount needs a neighbour table (nbor)");
     HEA_TRY(validate_problem(problem));
     const hea_problem *pb = problem;
     const int T = pb->num_types, S = pb->num_shells, N = pb->num_sites;
@@ -2043,6 +2114,11 @@ struct ServerRequest {
         p.species = const_cast<int32_t *>(species.data());
         p.weight = const_cast<double *>(weight.data());
         p.target_sro = const_cast<double *>(target.data());
+        if (lattice >= 0) {  // lattice requests keep no table: neighbours from lattice arithmetic
+            p.implicit_lattice = lattice + 1;
+            p.lattice_cell = cell;
+            p.lattice_shell_set = shell_set;
+        }
         return p;
     }
 };
@@ -2186,14 +2262,9 @@ int server_place(hea_server *sv, ServerRequest &r, int slot)
     SearchConst c;
     PadGeom g;
     fill_const(&pb, r.params.seed, c, g);
-    int raw_row = g.raw_row;
-    LatticeSpec sp{};
-    if (r.lattice >= 0) {
-        HEA_TRY(make_lattice_spec(r.lattice, r.shell_set, sp));
-        raw_row = sp.size[0] + sp.size[1] + sp.size[2];
-    }
+    const bool implicit = c.lat.L > 0;  // lattice requests: no table in the arena
     const int P = r.params.num_solutions;
-    const RequestLayout L = request_layout(c, g.pad_row, r.S, r.T, P);
+    const RequestLayout L = request_layout(c, implicit ? 0 : g.pad_row, r.S, r.T, P);
     if (sv->level_load[r.level] + 2ull * P > (unsigned long long)sv->cfg.ring_jobs) return HEA_PENDING;
     size_t off = 0;
     if (!sv->heap.alloc(L.total, &off)) return HEA_PENDING;
@@ -2201,34 +2272,30 @@ int server_place(hea_server *sv, ServerRequest &r, int slot)
     r.bytes = L.total;
     uint8_t *base = sv->arena + off;
 
-    // raw table (uploaded or built), then its padded, checked copy
-    const size_t raw = (size_t)r.N * raw_row * sizeof(int32_t);
-    int rc = sv->grow(&sv->d_raw, &sv->raw_bytes, raw);
-    if (rc != HEA_OK) {
-        sv->heap.release(off, L.total);
-        return rc;
-    }
+    // uploaded tables: the raw table, then its padded, checked copy; lattice requests: nothing
     cudaError_t e = cudaMemsetAsync(sv->d_err + slot, 0, sizeof(int), sv->stream);
-    if (e == cudaSuccess) {
-        if (r.lattice >= 0) {
-            const int blocks = (int)std::min<int64_t>(((int64_t)r.N + 255) / 256, 4096);
-            build_neighbors_kernel<<<blocks, 256, 0, sv->stream>>>(sp, r.cell, (int32_t *)sv->d_raw, raw_row,
-                                                                    sv->d_err + slot);
-            e = cudaGetLastError();
-        } else {
-            e = cudaMemcpyAsync(sv->d_raw, r.nbor.data(), raw, cudaMemcpyHostToDevice, sv->stream);
+    if (!implicit) {
+        const size_t raw = (size_t)r.N * g.raw_row * sizeof(int32_t);
+        int rc = sv->grow(&sv->d_raw, &sv->raw_bytes, raw);
+        if (rc != HEA_OK) {
+            sv->heap.release(off, L.total);
+            return rc;
         }
-    }
-    g.raw_row = raw_row;
-    if (e == cudaSuccess) {
-        pad_and_check_kernel<<<1184, 256, 0, sv->stream>>>((const int32_t *)sv->d_raw, (int32_t *)(base + L.nbor), g,
-                                                            sv->d_err + slot);
-        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(sv->d_raw, r.nbor.data(), raw, cudaMemcpyHostToDevice, sv->stream);
+        if (e == cudaSuccess) {
+            pad_and_check_kernel<<<1184, 256, 0, sv->stream>>>((const int32_t *)sv->d_raw,
+                                                                (int32_t *)(base + L.nbor), g, sv->d_err + slot);
+            e = cudaGetLastError();
+        }
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.nbmask, 0, L.hist - L.nbmask, sv->stream);
     if (e == cudaSuccess) {
-        nbmask_kernel<<<1184, 256, 0, sv->stream>>>((const int32_t *)(base + L.nbor), r.N, g.pad_row,
-                                                     (uint32_t *)(base + L.nbmask));
+        if (implicit)
+            nbmask_implicit_kernel<<<1184, 256, 0, sv->stream>>>(c, implicit_row(c, r.S),
+                                                                  (uint32_t *)(base + L.nbmask));
+        else
+            nbmask_kernel<<<1184, 256, 0, sv->stream>>>((const int32_t *)(base + L.nbor), r.N, g.pad_row,
+                                                         (uint32_t *)(base + L.nbmask));
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(base + L.occ, 0, L.cnt - L.occ, sv->stream);
@@ -2238,7 +2305,7 @@ int server_place(hea_server *sv, ServerRequest &r, int slot)
     }
     BatchStruct d{};
     d.c = c;
-    d.nbor = reinterpret_cast<const int4 *>(base + L.nbor);
+    d.nbor = implicit ? nullptr : reinterpret_cast<const int4 *>(base + L.nbor);
     d.occ = base + L.occ;
     d.cnt = reinterpret_cast<int32_t *>(base + L.cnt);
     d.f2 = reinterpret_cast<double *>(base + L.f2);
@@ -2445,7 +2512,7 @@ int server_enqueue(hea_server *sv, ServerRequest &&r, const hea_params *params, 
         SearchConst c;
         PadGeom g;
         fill_const(&pb, params->seed, c, g);
-        const RequestLayout L = request_layout(c, g.pad_row, r.S, r.T, params->num_solutions);
+        const RequestLayout L = request_layout(c, c.lat.L ? 0 : g.pad_row, r.S, r.T, params->num_solutions);
         if (L.total > sv->heap.total)
             return fail(HEA_ERR_UNSUPPORTED, "request needs %zu bytes of device memory; the arena holds %zu", L.total,
                         sv->heap.total);
@@ -2573,9 +2640,15 @@ int hea_server_submit(hea_server *server, const hea_problem *problem, const hea_
     r.species.assign(problem->species, problem->species + r.T);
     r.weight.assign(problem->weight, problem->weight + r.S);
     r.target.assign(problem->target_sro, problem->target_sro + (size_t)r.S * r.T * r.T);
-    int64_t row = 0;
-    for (int k = 0; k < r.S; ++k) row += r.shell_sizes[k];
-    r.nbor.assign(problem->nbor, problem->nbor + (size_t)r.N * row);
+    if (problem->nbor) {
+        int64_t row = 0;
+        for (int k = 0; k < r.S; ++k) row += r.shell_sizes[k];
+        r.nbor.assign(problem->nbor, problem->nbor + (size_t)r.N * row);
+    } else {  // implicit neighbours: the request keeps its lattice, no table
+        r.lattice = problem->implicit_lattice - 1;
+        r.cell = problem->lattice_cell;
+        r.shell_set = problem->lattice_shell_set;
+    }
     return server_enqueue(server, std::move(r), params, tolerance, priority, out_id);
 }
 

@@ -68,15 +68,21 @@ __global__ void __launch_bounds__(256) large_recount_kernel(const SearchConst c,
     uint4 *hs = hist ? hist + (size_t)slot * n : nullptr;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         const int a = row[s];
-        const int4 *r = nbor + (size_t)s * c.row4;
+        const SitePos ps = c.lat.L ? site_pos(c.lat, s) : SitePos{0, 0, 0};
         uint32_t hk[3] = {0u, 0u, 0u};
 #pragma unroll
         for (int k = 0; k < S; ++k) {
             uint32_t h = 0;
-            const int4 *seg = r + c.off4[k];
-            for (int ch = 0; ch < c.chunks[k]; ++ch) {
-                const int4 x = __ldg(seg + ch);
-                h += (1u << (5 * row[x.x])) + (1u << (5 * row[x.y])) + (1u << (5 * row[x.z])) + (1u << (5 * row[x.w]));
+            if (c.lat.L) {  // implicit neighbours (no sentinel padding: pad[k] == 0)
+                for (int v = 0; v < c.lat.zsize[k]; ++v)
+                    h += 1u << (5 * row[lattice_neighbor(c.lat, ps, c.lat.zoff[k] + v)]);
+            } else {
+                const int4 *seg = nbor + (size_t)s * c.row4 + c.off4[k];
+                for (int ch = 0; ch < c.chunks[k]; ++ch) {
+                    const int4 x = __ldg(seg + ch);
+                    h += (1u << (5 * row[x.x])) + (1u << (5 * row[x.y])) + (1u << (5 * row[x.z])) +
+                         (1u << (5 * row[x.w]));
+                }
             }
 #pragma unroll
             for (int t = 0; t < T; ++t) {

@@ -17,6 +17,24 @@
 
 namespace hea {
 
+// Implicit neighbour ids of a perfect FCC/BCC cube (the structure keeps no
+// neighbour table in memory).  Site s = nb (x L^2 + y L + z) + basis, position
+// in half lattice units 2 (x, y, z) + basis offset; the e-th neighbour of s
+// (shells concatenated) is the site at position(s) + vec[e], periodic in every
+// axis -- the same sites, in another order within each shell, as the table of
+// pyhea/lattice/lattice.py:196-323 (the order within a shell does not enter
+// any count or histogram).
+struct LatticeConst {
+    int32_t L;                   // cube edge in cells; 0: the structure has a neighbour table
+    int32_t nb;                  // basis sites per cell (4 FCC, 2 BCC)
+    int32_t zsize[3], zoff[3];   // shell sizes and their offsets into vec
+    int8_t basis[4][3];          // basis offsets, half units
+    int8_t vec[54][3];           // neighbour offsets, half units, shells concatenated
+    int8_t lut[8];               // basis index by position parity (x&1)*4 + (y&1)*2 + (z&1); -1: none
+    int8_t pad_[2];
+};
+static_assert(sizeof(LatticeConst) % 8 == 0, "LatticeConst keeps SearchConst 8-byte sized");
+
 struct SearchConst {
     double E[kMaxShells * kMaxTypes * kMaxTypes];  // 1 - target, [S][T][T] compact
     double R[kMaxShells * kMaxTypes * kMaxTypes];  // N / (Z_k n_i n_j), [S][T][T] compact
@@ -29,7 +47,36 @@ struct SearchConst {
     uint32_t reject_below, key0, key1;
     uint32_t draw16;    // 1: 16-bit draws, four attempts per Philox call (use_draw16)
     uint32_t reject16;  // 2^16 mod N
+    LatticeConst lat;   // lat.L > 0: neighbours from lattice arithmetic (nbor unused)
 };
+
+struct SitePos {
+    int x, y, z;
+};
+
+// Position of site s in half lattice units.
+__device__ __forceinline__ SitePos site_pos(const LatticeConst &lc, int s)
+{
+    const int b = s & (lc.nb - 1), cell = s >> (lc.nb == 4 ? 2 : 1);  // nb is 2 or 4
+    const int LL = lc.L * lc.L, cx = cell / LL, r = cell - cx * LL, cy = r / lc.L, cz = r - cy * lc.L;
+    return SitePos{2 * cx + lc.basis[b][0], 2 * cy + lc.basis[b][1], 2 * cz + lc.basis[b][2]};
+}
+
+// The e-th neighbour (shells concatenated) of the site at position p.  Offsets
+// are at most 2 half units, so one wrap per axis keeps q in [0, 2L).
+__device__ __forceinline__ int lattice_neighbor(const LatticeConst &lc, const SitePos &p, int e)
+{
+    const int M = 2 * lc.L;
+    int qx = p.x + lc.vec[e][0], qy = p.y + lc.vec[e][1], qz = p.z + lc.vec[e][2];
+    qx += qx < 0 ? M : 0;
+    qy += qy < 0 ? M : 0;
+    qz += qz < 0 ? M : 0;
+    qx -= qx >= M ? M : 0;
+    qy -= qy >= M ? M : 0;
+    qz -= qz >= M ? M : 0;
+    const int bi = lc.lut[((qx & 1) << 2) | ((qy & 1) << 1) | (qz & 1)];
+    return lc.nb * (((qx >> 1) * lc.L + (qy >> 1)) * lc.L + (qz >> 1)) + bi;
+}
 
 // Shell layout of the padded table, in int4 chunks per shell (0: shell absent).
 // Fixed layouts unroll every load; RuntimeShells reads the chunk counts from
@@ -233,15 +280,26 @@ __device__ __forceinline__ double score_delta(const SearchConst &c, const int4 *
     }
     const int a5 = 5 * a, b5 = 5 * b;
     if (near) {
-        const int row4 = L::kRuntime ? c.row4 : L::kRow4;
-        const int4 *r1 = nbor + (size_t)s1 * row4;
+        if (c.lat.L) {  // implicit neighbours
+            const SitePos p1 = site_pos(c.lat, (int)s1);
 #pragma unroll
-        for (int k = 0; k < S; ++k) {
-            const int o = L::kRuntime ? c.off4[k] : L::off(k), n = L::kRuntime ? c.chunks[k] : L::chunks(k);
-            uint32_t m = 0;
-            for (int ch = 0; ch < n; ++ch) m += count4(__ldg(r1 + o + ch), s2);
-            h1[k] += m << a5;
-            h2[k] += m << b5;
+            for (int k = 0; k < S; ++k) {
+                uint32_t m = 0;
+                for (int v = 0; v < c.lat.zsize[k]; ++v) m += lattice_neighbor(c.lat, p1, c.lat.zoff[k] + v) == (int)s2;
+                h1[k] += m << a5;
+                h2[k] += m << b5;
+            }
+        } else {
+            const int row4 = L::kRuntime ? c.row4 : L::kRow4;
+            const int4 *r1 = nbor + (size_t)s1 * row4;
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const int o = L::kRuntime ? c.off4[k] : L::off(k), n = L::kRuntime ? c.chunks[k] : L::chunks(k);
+                uint32_t m = 0;
+                for (int ch = 0; ch < n; ++ch) m += count4(__ldg(r1 + o + ch), s2);
+                h1[k] += m << a5;
+                h2[k] += m << b5;
+            }
         }
     }
     const double2 *row = tab + (a * T + b) * R;
@@ -274,9 +332,21 @@ template <class L, bool kSpeciesWord>
 __device__ __forceinline__ void update_hist(const SearchConst &c, const int4 *__restrict__ nbor, uint4 *hist,
                                             uint32_t s1, uint32_t s2, int a, int b, int me)
 {
+    const uint32_t up = (1u << (5 * b)) - (1u << (5 * a));  // s1's neighbours: one a becomes b
+    if (c.lat.L) {  // implicit neighbours: row e of s1 then of s2, shells concatenated
+        const int row = c.lat.zoff[L::S - 1] + c.lat.zsize[L::S - 1];
+        for (int e = me; e < 2 * row; e += blockDim.x) {
+            const bool first = e < row;
+            const int idx = first ? e : e - row;
+            const int n = lattice_neighbor(c.lat, site_pos(c.lat, (int)(first ? s1 : s2)), idx);
+            int k = 0;
+#pragma unroll
+            for (int kk = 1; kk < L::S; ++kk) k += idx >= c.lat.zoff[kk];
+            atomicAdd(reinterpret_cast<uint32_t *>(hist + n) + k, first ? up : 0u - up);
+        }
+    } else {
     const int row4 = L::kRuntime ? c.row4 : L::kRow4;
     const int row = 4 * row4;
-    const uint32_t up = (1u << (5 * b)) - (1u << (5 * a));  // s1's neighbours: one a becomes b
     for (int e = me; e < 2 * row; e += blockDim.x) {
         const bool first = e < row;
         const int idx = first ? e : e - row;
@@ -288,6 +358,7 @@ __device__ __forceinline__ void update_hist(const SearchConst &c, const int4 *__
         for (int kk = 1; kk < L::S; ++kk) k += idx >= 4 * (L::kRuntime ? c.off4[kk] : L::off(kk));
         uint32_t *h = reinterpret_cast<uint32_t *>(hist + n) + k;
         atomicAdd(h, first ? up : 0u - up);
+    }
     }
     if (kSpeciesWord && me == 0) {
         hist[s1].w = (uint32_t)(5 * b);
@@ -447,16 +518,21 @@ __device__ void block_recount(const SearchConst &c, const int4 *__restrict__ nbo
     int since = 0;
     for (int s = threadIdx.x; s < c.num_sites; s += blockDim.x) {
         const int a5 = occ5[s];
-        const int4 *row = nbor + (size_t)s * c.row4;
+        const SitePos ps = c.lat.L ? site_pos(c.lat, s) : SitePos{0, 0, 0};
         uint32_t hs[3] = {0u, 0u, 0u};
 #pragma unroll
         for (int k = 0; k < S; ++k) {
             uint64_t h = 0;
-            const int4 *seg = row + c.off4[k];
-            for (int ch = 0; ch < c.chunks[k]; ++ch) {
-                const int4 x = __ldg(seg + ch);
-                h += (1ull << (2 * occ5[x.x])) + (1ull << (2 * occ5[x.y])) + (1ull << (2 * occ5[x.z])) +
-                     (1ull << (2 * occ5[x.w]));
+            if (c.lat.L) {  // implicit neighbours (no sentinel padding: pad[k] == 0)
+                for (int v = 0; v < c.lat.zsize[k]; ++v)
+                    h += 1ull << (2 * occ5[lattice_neighbor(c.lat, ps, c.lat.zoff[k] + v)]);
+            } else {
+                const int4 *seg = nbor + (size_t)s * c.row4 + c.off4[k];
+                for (int ch = 0; ch < c.chunks[k]; ++ch) {
+                    const int4 x = __ldg(seg + ch);
+                    h += (1ull << (2 * occ5[x.x])) + (1ull << (2 * occ5[x.y])) + (1ull << (2 * occ5[x.z])) +
+                         (1ull << (2 * occ5[x.w]));
+                }
             }
 #pragma unroll
             for (int i = 0; i < T; ++i)

@@ -93,9 +93,14 @@ class Structure:
     def shell_sizes(self):
         return _lat.shell_vectors(self.lattice, self.shell_set)
 
-    def problem(self, device=False):
+    def problem(self, device=False, implicit=False):
+        """Problem with the neighbour table (built on the device when `device`), or, with
+        `implicit`, the lattice description instead of a table."""
         from . import Problem
 
+        if implicit:
+            return Problem.from_lattice(self.lattice, self.cell, self.species, self.weight, self.target,
+                                        shell_set=self.shell_set)
         nbor, sizes = self.neighbors(device)
         return Problem(nbor, sizes, self.species, self.weight, self.target)
 
