@@ -117,6 +117,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="headline line only (no batched/serving/large)")
     ap.add_argument("--cpu-procs", type=int, default=0, help="reference processes (0: all host cores)")
+    ap.add_argument("--neighbours", choices=["table", "implicit"], default="table",
+                    help="batched, large and --case: neighbour table or implicit lattice neighbours")
     ap.add_argument("--case", choices=["plain", "batch", "large"], help="one small case for a profiler capture")
     ap.add_argument("--iters", type=int, default=1, help="--case plain/batch: iterations")
     ap.add_argument("--count", type=int, default=16, help="--case batch: structures")
@@ -307,7 +309,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # Batched: the mixed 64-structure batch
 # ---------------------------------------------------------------------------
-def measure_batched(steps, warmup, l2_peak=None):
+def measure_batched(steps, warmup, l2_peak=None, implicit=False):
     """64 structures (FCC/BCC, edge 6..30, 3-6 species, Dirichlet(2) compositions), 64 solutions x
     256 tasks, 10 iterations, depth 10.  value = swap evaluations/s of the batched persistent kernel;
     plain = the same structures searched one structure per launch sequence (device-resident plans,
@@ -319,7 +321,7 @@ def measure_batched(steps, warmup, l2_peak=None):
     from pyhea_b200 import workloads as W
 
     structs = W.batched(seed=0)
-    problems = [st.problem(device=True) for st in structs]
+    problems = [st.problem(device=True, implicit=implicit) for st in structs]
     params = [dict(num_solutions=st.P, total_iter=st.I, parallel_task=st.Q, converge_depth=st.D) for st in structs]
     seeds = lambda k: [7919 * k + i for i in range(len(structs))]  # noqa: E731
     batch = hb.Batch(problems, params)
@@ -412,7 +414,8 @@ def run_batched(args):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     import pyhea_b200 as hb
 
-    sub = measure_batched(args.steps, args.warmup, hb.l2_read_probe(L2_PROBE_BYTES))
+    sub = measure_batched(args.steps, args.warmup, hb.l2_read_probe(L2_PROBE_BYTES),
+                          implicit=args.neighbours == "implicit")
     line = {"metric": "swap_evals_per_sec", "n_gpus": 1, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
     line.update(sub)
@@ -423,10 +426,11 @@ def run_batched(args):
 # ---------------------------------------------------------------------------
 # Large: FCC 100^3
 # ---------------------------------------------------------------------------
-def measure_large(iters, e2e=True):
+def measure_large(iters, e2e=True, implicit=False):
     """FCC 100^3 (4,000,000 sites, 12/6/24 shells, 672 MB neighbour table), 4 species at 0.25, 32
     solutions x 4096 tasks, depth 20: `iters` iterations of the uncapped search (the configuration
-    states 200).  Occupancies stay in HBM; each solution runs on a thread-block cluster."""
+    states 200).  Occupancies stay in HBM; each solution runs on a thread-block cluster.  With
+    `implicit` the neighbour ids come from lattice arithmetic and no table is uploaded or read."""
     import numpy as np
     import torch
 
@@ -434,7 +438,7 @@ def measure_large(iters, e2e=True):
     from pyhea_b200 import workloads as W
 
     st = W.large(seed=0)
-    pb = st.problem(device=True)
+    pb = st.problem(device=True, implicit=implicit)
     warm = hb.Plan(pb, st.P, 1, st.Q, st.D, max_rounds=50)  # kernels loaded; capped
     warm.run(0)
     warm.close()
@@ -451,7 +455,8 @@ def measure_large(iters, e2e=True):
                       "parallel_task": st.Q, "converge_depth": st.D, "total_iter_run": iters,
                       "total_iter_stated": st.I, "max_rounds_per_local_search": None,
                       "warmup": "one capped (50-round) iteration",
-                      "l2": "inputs larger than L2 (704 MB table)"},
+                      "neighbours": "implicit (lattice arithmetic, no table)" if implicit else "table",
+                      "l2": "inputs larger than L2 (4.1 GB of site histograms)"},
            "clocks": clocks}
     peak, peak_kind = measured_peaks()
     B = st.evals_bytes()
@@ -466,14 +471,19 @@ def measure_large(iters, e2e=True):
         # end to end through the C ABI with pinned host buffers: the neighbour table uploaded and the
         # population read back (same seed as the device-timed step, so the same work)
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
-        hp = hb.Problem(pin(pb.nbor), pin(pb.shell_sizes), pin(pb.species), pin(pb.weight), pin(pb.target_sro))
+        if implicit:
+            hp = hb.Problem(None, pin(pb.shell_sizes), pin(pb.species), pin(pb.weight), pin(pb.target_sro),
+                            lattice=pb.lattice)
+        else:
+            hp = hb.Problem(pin(pb.nbor), pin(pb.shell_sizes), pin(pb.species), pin(pb.weight),
+                            pin(pb.target_sro))
         out_occ = torch.empty((st.P, st.num_sites), dtype=torch.uint8).pin_memory().numpy()
         out_fit = torch.empty(st.P, dtype=torch.float64).pin_memory().numpy()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         _, _, e = hb.search(hp, st.P, iters, st.Q, st.D, seed=1, out_occ=out_occ, out_fitness=out_fit)
         dt = time.perf_counter() - t0
-        h2d = hp.nbor.nbytes + hp.shell_sizes.nbytes + hp.species.nbytes + hp.weight.nbytes + hp.target_sro.nbytes
+        h2d = (hp.nbor.nbytes if hp.nbor is not None else 0) + hp.shell_sizes.nbytes + hp.species.nbytes + hp.weight.nbytes + hp.target_sro.nbytes
         out["e2e"] = {"value": e["evals"] / dt, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
                       "d2h_bytes_per_step": int(out_occ.nbytes + out_fit.nbytes)}
     return out
@@ -485,7 +495,7 @@ def run_large(args):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     line = {"metric": "swap_evals_per_sec", "n_gpus": 1, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
-    line.update(measure_large(args.large_iters))
+    line.update(measure_large(args.large_iters, implicit=args.neighbours == "implicit"))
     print(json.dumps(line))
     return 0
 
@@ -689,14 +699,15 @@ def run_case(args):
     from pyhea_b200 import lattice as L
     from pyhea_b200 import workloads as W
 
+    implicit = args.neighbours == "implicit"
     if args.case == "plain":
         st = W.plain_gpu(seed=0)
-        plan = hb.Plan(st.problem(device=True), st.P, args.iters, st.Q, st.D)
+        plan = hb.Plan(st.problem(device=True, implicit=implicit), st.P, args.iters, st.Q, st.D)
         out = plan.run(123)
         plan.close()
     elif args.case == "batch":
         structs = sorted(W.batched(seed=0), key=lambda s: -s.num_sites)[: args.count]
-        problems = [st.problem(device=True) for st in structs]
+        problems = [st.problem(device=True, implicit=implicit) for st in structs]
         params = [dict(num_solutions=st.P, total_iter=args.iters, parallel_task=st.Q, converge_depth=st.D)
                   for st in structs]
         b = hb.Batch(problems, params)
@@ -707,7 +718,8 @@ def run_case(args):
         n = 4 * args.cell ** 3
         st = W.Structure(L.FCC, args.cell, L.SHELLS_FCC_TRUE3, [n // 4] * 4, W.WEIGHTS,
                          W.zero_row_sum_target(rng, 4, 0.05), P=32, Q=4096, I=1, D=20, name=f"fcc{args.cell}")
-        plan = hb.Plan(st.problem(device=True), st.P, 1, st.Q, st.D, max_rounds=args.rounds, hbm_occupancy=True)
+        plan = hb.Plan(st.problem(device=True, implicit=implicit), st.P, 1, st.Q, st.D, max_rounds=args.rounds,
+                       hbm_occupancy=True)
         out = plan.run(123)
         plan.close()
     print(json.dumps(out))

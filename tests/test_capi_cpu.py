@@ -94,3 +94,22 @@ def test_reference_driver_call_is_accepted():
     with pytest.raises(RuntimeError) as err:
         accelerate.run_local_parallel_hcs_cuda(*args)
     assert not isinstance(err.value, (TypeError, ValueError))
+
+
+@pytest.mark.parametrize("lattice,cell,species,shell_set,msg", [
+    (L.FCC, 4, (64, 64, 64, 60), L.SHELLS_REFERENCE, "does not hold"),   # 252 sites, not 4 * 4^3
+    (L.BCC, 1, (1, 1), L.SHELLS_REFERENCE, "does not hold"),             # edge below 2
+])
+def test_implicit_lattice_must_describe_the_structure(lattice, cell, species, shell_set, msg):
+    """An implicit-neighbour problem is checked against its lattice before any device work."""
+    T = len(species)
+    pb = hb.Problem.from_lattice(lattice, cell, species, [4.0, 1.0, 0.5], np.zeros((3, T * T)), shell_set=shell_set)
+    with pytest.raises(ValueError, match=msg):
+        hb.search(pb, 2, 1, 8, 2)
+
+
+def test_implicit_lattice_shell_sizes_must_match():
+    pb = hb.Problem.from_lattice(L.FCC, 4, (64,) * 4, [4.0, 1.0, 0.5], np.zeros((3, 16)))
+    pb.shell_sizes[2] = 24  # the reference shell set's third FCC shell has 12
+    with pytest.raises(ValueError, match="shell 2"):
+        hb.search(pb, 2, 1, 8, 2)
