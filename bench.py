@@ -309,6 +309,24 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # Batched: the mixed 64-structure batch
 # ---------------------------------------------------------------------------
+def pinned_problem(pb):
+    """The same problem with its host arrays in pinned memory (implicit problems keep no table)."""
+    import numpy as np
+    import torch
+
+    import pyhea_b200 as hb
+
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    return hb.Problem(None if pb.nbor is None else pin(pb.nbor), pin(pb.shell_sizes), pin(pb.species),
+                      pin(pb.weight), pin(pb.target_sro), lattice=pb.lattice)
+
+
+def problem_bytes(pb):
+    """Host bytes a search copies to the device for a problem."""
+    return ((pb.nbor.nbytes if pb.nbor is not None else 0) + pb.shell_sizes.nbytes + pb.species.nbytes +
+            pb.weight.nbytes + pb.target_sro.nbytes)
+
+
 def measure_batched(steps, warmup, l2_peak=None, implicit=False):
     """64 structures (FCC/BCC, edge 6..30, 3-6 species, Dirichlet(2) compositions), 64 solutions x
     256 tasks, 10 iterations, depth 10.  value = swap evaluations/s of the batched persistent kernel;
@@ -359,12 +377,9 @@ def measure_batched(steps, warmup, l2_peak=None, implicit=False):
 
     # end to end through the public API: every step creates the batch from the host problems in
     # pinned memory (tables uploaded), runs it and reads every structure's population back
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
-    pinned = [hb.Problem(pin(pb.nbor), pin(pb.shell_sizes), pin(pb.species), pin(pb.weight), pin(pb.target_sro))
-              for pb in problems]
+    pinned = [pinned_problem(pb) for pb in problems]
     e2e_s, e2e_ev = 0.0, 0
-    h2d = sum(pb.nbor.nbytes + pb.shell_sizes.nbytes + pb.species.nbytes + pb.weight.nbytes + pb.target_sro.nbytes
-              for pb in pinned)
+    h2d = sum(problem_bytes(pb) for pb in pinned)
     d2h = sum(st.P * (st.num_sites + 8) for st in structs)
     for k in range(steps):
         flush.zero_()
@@ -470,20 +485,14 @@ def measure_large(iters, e2e=True, implicit=False):
     if e2e:
         # end to end through the C ABI with pinned host buffers: the neighbour table uploaded and the
         # population read back (same seed as the device-timed step, so the same work)
-        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
-        if implicit:
-            hp = hb.Problem(None, pin(pb.shell_sizes), pin(pb.species), pin(pb.weight), pin(pb.target_sro),
-                            lattice=pb.lattice)
-        else:
-            hp = hb.Problem(pin(pb.nbor), pin(pb.shell_sizes), pin(pb.species), pin(pb.weight),
-                            pin(pb.target_sro))
+        hp = pinned_problem(pb)
         out_occ = torch.empty((st.P, st.num_sites), dtype=torch.uint8).pin_memory().numpy()
         out_fit = torch.empty(st.P, dtype=torch.float64).pin_memory().numpy()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         _, _, e = hb.search(hp, st.P, iters, st.Q, st.D, seed=1, out_occ=out_occ, out_fitness=out_fit)
         dt = time.perf_counter() - t0
-        h2d = (hp.nbor.nbytes if hp.nbor is not None else 0) + hp.shell_sizes.nbytes + hp.species.nbytes + hp.weight.nbytes + hp.target_sro.nbytes
+        h2d = problem_bytes(hp)
         out["e2e"] = {"value": e["evals"] / dt, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
                       "d2h_bytes_per_step": int(out_occ.nbytes + out_fit.nbytes)}
     return out

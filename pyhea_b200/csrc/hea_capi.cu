@@ -538,6 +538,7 @@ void fill_lattice_const(const hea_problem *pb, SearchConst &c)
     for (int q = 0; q < 8; ++q) lc.lut[q] = -1;
     for (int b = 0; b < sp.nb; ++b)
         lc.lut[((sp.basis[b][0] & 1) << 2) | ((sp.basis[b][1] & 1) << 1) | (sp.basis[b][2] & 1)] = (int8_t)b;
+    lc.kind = (int8_t)(pb->implicit_lattice == 2 ? kLatBcc : pb->lattice_shell_set == 1 ? kLatFccTrue3 : kLatFccRef);
     for (int k = 0; k < kMaxShells; ++k) c.pad[k] = 0;  // no sentinel padding in computed rows
 }
 

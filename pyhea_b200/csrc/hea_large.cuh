@@ -66,32 +66,39 @@ __global__ void __launch_bounds__(256) large_recount_kernel(const SearchConst c,
     __syncthreads();
     const int n = c.num_sites;
     uint4 *hs = hist ? hist + (size_t)slot * n : nullptr;
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    // one site with its shell histograms h (5-bit fields)
+    const auto site = [&](int s, const uint32_t (&h)[S]) {
         const int a = row[s];
-        const SitePos ps = c.lat.L ? site_pos(c.lat, s) : SitePos{0, 0, 0};
         uint32_t hk[3] = {0u, 0u, 0u};
 #pragma unroll
         for (int k = 0; k < S; ++k) {
-            uint32_t h = 0;
-            if (c.lat.L) {  // implicit neighbours (no sentinel padding: pad[k] == 0)
-                for (int v = 0; v < c.lat.zsize[k]; ++v)
-                    h += 1u << (5 * row[lattice_neighbor(c.lat, ps, c.lat.zoff[k] + v)]);
-            } else {
+#pragma unroll
+            for (int t = 0; t < T; ++t) {
+                const int v = (int)((h[k] >> (5 * t)) & 31u);
+                if (v) atomicAdd(&bins[(k * T + a) * T + t], v);
+            }
+            hk[k] = h[k] - (uint32_t)c.pad[k];  // sentinel entries counted as species 0
+        }
+        if (hs) hs[s] = make_uint4(hk[0], hk[1], hk[2], (uint32_t)(5 * a));  // species word: 5*species
+    };
+    const int first = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    if (c.lat.L) {  // implicit neighbours (no sentinel padding: pad[k] == 0)
+        lattice_sites<S, uint32_t>(c.lat, first, stride, [row](int n) { return 1u << (5 * row[n]); }, site);
+    } else {
+        for (int s = first; s < n; s += stride) {
+            uint32_t h[S];
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                h[k] = 0;
                 const int4 *seg = nbor + (size_t)s * c.row4 + c.off4[k];
                 for (int ch = 0; ch < c.chunks[k]; ++ch) {
                     const int4 x = __ldg(seg + ch);
-                    h += (1u << (5 * row[x.x])) + (1u << (5 * row[x.y])) + (1u << (5 * row[x.z])) +
-                         (1u << (5 * row[x.w]));
+                    h[k] += (1u << (5 * row[x.x])) + (1u << (5 * row[x.y])) + (1u << (5 * row[x.z])) +
+                            (1u << (5 * row[x.w]));
                 }
             }
-#pragma unroll
-            for (int t = 0; t < T; ++t) {
-                const int v = (int)((h >> (5 * t)) & 31u);
-                if (v) atomicAdd(&bins[(k * T + a) * T + t], v);
-            }
-            hk[k] = h - (uint32_t)c.pad[k];  // sentinel entries counted as species 0
+            site(s, h);
         }
-        if (hs) hs[s] = make_uint4(hk[0], hk[1], hk[2], (uint32_t)(5 * a));  // species word: 5*species
     }
     __syncthreads();
     int32_t *g = cnt + (size_t)slot * S * T * T;

@@ -12,6 +12,7 @@
 // 5-bit histogram field), plus the sentinel byte 0 at index N.
 #pragma once
 #include <cstdint>
+#include <utility>
 
 #include "hea_device.cuh"
 
@@ -31,7 +32,8 @@ struct LatticeConst {
     int8_t basis[4][3];          // basis offsets, half units
     int8_t vec[54][3];           // neighbour offsets, half units, shells concatenated
     int8_t lut[8];               // basis index by position parity (x&1)*4 + (y&1)*2 + (z&1); -1: none
-    int8_t pad_[2];
+    int8_t kind;                 // kLatFccRef, kLatFccTrue3 or kLatBcc (lattice_sites)
+    int8_t pad_;
 };
 static_assert(sizeof(LatticeConst) % 8 == 0, "LatticeConst keeps SearchConst 8-byte sized");
 
@@ -76,6 +78,158 @@ __device__ __forceinline__ int lattice_neighbor(const LatticeConst &lc, const Si
     qz -= qz >= M ? M : 0;
     const int bi = lc.lut[((qx & 1) << 2) | ((qy & 1) << 1) | (qz & 1)];
     return lc.nb * (((qx >> 1) * lc.L + (qy >> 1)) * lc.L + (qz >> 1)) + bi;
+}
+
+// Compile-time geometry of the three implicit lattices, for the walks over
+// every site (recounts).  A neighbour of a site of basis b in cell (cx, cy, cz)
+// lies in cell (cx + dx, cy + dy, cz + dz), d in {-1, 0, 1}, at basis b'; with
+// (kind, b, shell, entry) known at compile time its id is one sum of three
+// per-site axis terms (LatticeAxes) and b'.  Shell generators in half units:
+// FCC (1,1,0) 12, (2,0,0) 6, then (2,2,0) 12 (reference set) or (2,1,1) 24
+// (true third shell); BCC (1,1,1) 8, (2,0,0) 6, (2,2,0) 12 -- the sets of
+// lattice_neighbor, entries in another order.
+enum : int { kLatFccRef = 0, kLatFccTrue3 = 1, kLatBcc = 2 };
+
+__host__ __device__ constexpr int lat_nb(int kind) { return kind == kLatBcc ? 2 : 4; }
+__host__ __device__ constexpr int lat_basis(int kind, int b, int d)
+{
+    // FCC {0,0,0} {1,1,0} {1,0,1} {0,1,1}; BCC {0,0,0} {1,1,1}
+    return kind == kLatBcc ? b : (b == 0 ? 0 : (d == 0 ? (b != 3) : d == 1 ? (b != 2) : (b != 1)));
+}
+__host__ __device__ constexpr int lat_gen(int kind, int k, int d)
+{
+    return k == 0 ? (kind == kLatBcc ? 1 : (d < 2 ? 1 : 0))
+         : k == 1 ? (d == 0 ? 2 : 0)
+         : (kind == kLatFccTrue3 ? (d == 0 ? 2 : 1) : (d < 2 ? 2 : 0));
+}
+__host__ __device__ constexpr int lat_shell_size(int kind, int k)
+{
+    return k == 0 ? (kind == kLatBcc ? 8 : 12) : k == 1 ? 6 : (kind == kLatFccTrue3 ? 24 : 12);
+}
+// Component d of the i-th signed permutation of shell k's generator (48 candidates, duplicates included).
+__host__ __device__ constexpr int lat_candidate(int kind, int k, int i, int d)
+{
+    const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+    const int sgn = ((i >> (2 - d)) & 1) ? -1 : 1;  // i = 8 p + (sx sy sz)
+    return sgn * lat_gen(kind, k, perm[i >> 3][d]);
+}
+// Packed descriptor of entry e of shell k for basis b: (dx+1) | (dy+1) << 2 | (dz+1) << 4 | b' << 6.
+__host__ __device__ constexpr int lat_desc(int kind, int b, int k, int e)
+{
+    int seen = -1, pick = 0;
+    for (int i = 0; i < 48 && seen < e; ++i) {
+        bool dup = false;
+        for (int j = 0; j < i && !dup; ++j)
+            dup = lat_candidate(kind, k, j, 0) == lat_candidate(kind, k, i, 0) &&
+                  lat_candidate(kind, k, j, 1) == lat_candidate(kind, k, i, 1) &&
+                  lat_candidate(kind, k, j, 2) == lat_candidate(kind, k, i, 2);
+        if (!dup) {
+            ++seen;
+            pick = i;
+        }
+    }
+    int out = 0, par[3] = {0, 0, 0};
+    for (int d = 0; d < 3; ++d) {
+        const int q = lat_basis(kind, b, d) + lat_candidate(kind, k, pick, d);  // -2 .. 3
+        const int cell = q >= 0 ? q / 2 : -1;
+        par[d] = q & 1;
+        out |= (cell + 1) << (2 * d);
+    }
+    int bp = 0;
+    for (int x = 0; x < lat_nb(kind); ++x)
+        if (lat_basis(kind, x, 0) == par[0] && lat_basis(kind, x, 1) == par[1] && lat_basis(kind, x, 2) == par[2])
+            bp = x;
+    return out | (bp << 6);
+}
+
+// Per-site axis terms: x[d] = nb L^2 wrap(cx + d - 1), y[d] = nb L wrap(cy + d - 1), z[d] = nb wrap(cz + d - 1).
+struct LatticeAxes {
+    int x[3], y[3], z[3];
+};
+
+__device__ __forceinline__ LatticeAxes lattice_axes(int L, int nb, int cx, int cy, int cz)
+{
+    const int sx = nb * L * L, sy = nb * L;
+    LatticeAxes a;
+    a.x[0] = (cx == 0 ? L - 1 : cx - 1) * sx;
+    a.x[1] = cx * sx;
+    a.x[2] = (cx == L - 1 ? 0 : cx + 1) * sx;
+    a.y[0] = (cy == 0 ? L - 1 : cy - 1) * sy;
+    a.y[1] = cy * sy;
+    a.y[2] = (cy == L - 1 ? 0 : cy + 1) * sy;
+    a.z[0] = (cz == 0 ? L - 1 : cz - 1) * nb;
+    a.z[1] = cz * nb;
+    a.z[2] = (cz == L - 1 ? 0 : cz + 1) * nb;
+    return a;
+}
+
+template <int D>
+__device__ __forceinline__ int lat_id(const LatticeAxes &a)
+{
+    return a.x[D & 3] + a.y[(D >> 2) & 3] + a.z[(D >> 4) & 3] + (D >> 6);
+}
+
+template <int Kind, int B, int K, class H, class W, int... E>
+__device__ __forceinline__ H lat_shell_sum(const LatticeAxes &a, W &weight, std::integer_sequence<int, E...>)
+{
+    return (H(0) + ... + weight(lat_id<lat_desc(Kind, B, K, E)>(a)));
+}
+
+// Cells first, first + stride, ... of basis B: site(s, h) with h[k] = sum of
+// weight(n) over the shell-k neighbours n of site s.
+template <int Kind, int B, int S, class H, class W, class F>
+__device__ __forceinline__ void lattice_walk(int L, int first, int stride, W &weight, F &site)
+{
+    constexpr int NB = lat_nb(Kind);
+    const int LL = L * L, ncell = LL * L;
+    int cell = first;
+    int cx = cell / LL, cy = (cell - cx * LL) / L, cz = cell - cx * LL - cy * L;
+    const int bx = stride / LL, by = (stride - bx * LL) / L, bz = stride - bx * LL - by * L;
+    for (; cell < ncell; cell += stride) {
+        const LatticeAxes a = lattice_axes(L, NB, cx, cy, cz);
+        H h[S];
+        h[0] = lat_shell_sum<Kind, B, 0, H>(a, weight, std::make_integer_sequence<int, lat_shell_size(Kind, 0)>{});
+        if constexpr (S > 1)
+            h[1] = lat_shell_sum<Kind, B, 1, H>(a, weight, std::make_integer_sequence<int, lat_shell_size(Kind, 1)>{});
+        if constexpr (S > 2)
+            h[2] = lat_shell_sum<Kind, B, 2, H>(a, weight, std::make_integer_sequence<int, lat_shell_size(Kind, 2)>{});
+        site(NB * cell + B, h);
+        cz += bz;  // next cell of the walk: cell += stride in (cx, cy, cz) digits
+        if (cz >= L) {
+            cz -= L;
+            ++cy;
+        }
+        cy += by;
+        if (cy >= L) {
+            cy -= L;
+            ++cx;
+        }
+        cx += bx;
+    }
+}
+
+// Every site of an implicit lattice (this thread's share of a walk that
+// starts at cell `first` and steps by `stride` cells, once per basis index, so
+// that the threads of a warp share the basis and the neighbour geometry is
+// compile-time): site(s, h[S]) with h[k] = sum of weight(n) over the shell-k
+// neighbours n of s.
+template <int S, class H, class W, class F>
+__device__ __forceinline__ void lattice_sites(const LatticeConst &lc, int first, int stride, W weight, F site)
+{
+    if (lc.kind == kLatBcc) {
+        lattice_walk<kLatBcc, 0, S, H>(lc.L, first, stride, weight, site);
+        lattice_walk<kLatBcc, 1, S, H>(lc.L, first, stride, weight, site);
+    } else if (lc.kind == kLatFccTrue3) {
+        lattice_walk<kLatFccTrue3, 0, S, H>(lc.L, first, stride, weight, site);
+        lattice_walk<kLatFccTrue3, 1, S, H>(lc.L, first, stride, weight, site);
+        lattice_walk<kLatFccTrue3, 2, S, H>(lc.L, first, stride, weight, site);
+        lattice_walk<kLatFccTrue3, 3, S, H>(lc.L, first, stride, weight, site);
+    } else {
+        lattice_walk<kLatFccRef, 0, S, H>(lc.L, first, stride, weight, site);
+        lattice_walk<kLatFccRef, 1, S, H>(lc.L, first, stride, weight, site);
+        lattice_walk<kLatFccRef, 2, S, H>(lc.L, first, stride, weight, site);
+        lattice_walk<kLatFccRef, 3, S, H>(lc.L, first, stride, weight, site);
+    }
 }
 
 // Shell layout of the padded table, in int4 chunks per shell (0: shell absent).
@@ -516,33 +670,40 @@ __device__ void block_recount(const SearchConst &c, const int4 *__restrict__ nbo
             }
     };
     int since = 0;
-    for (int s = threadIdx.x; s < c.num_sites; s += blockDim.x) {
+    // one site with its shell histograms h (10-bit fields)
+    const auto site = [&](int s, const uint64_t (&h)[S]) {
         const int a5 = occ5[s];
-        const SitePos ps = c.lat.L ? site_pos(c.lat, s) : SitePos{0, 0, 0};
         uint32_t hs[3] = {0u, 0u, 0u};
 #pragma unroll
         for (int k = 0; k < S; ++k) {
-            uint64_t h = 0;
-            if (c.lat.L) {  // implicit neighbours (no sentinel padding: pad[k] == 0)
-                for (int v = 0; v < c.lat.zsize[k]; ++v)
-                    h += 1ull << (2 * occ5[lattice_neighbor(c.lat, ps, c.lat.zoff[k] + v)]);
-            } else {
-                const int4 *seg = nbor + (size_t)s * c.row4 + c.off4[k];
-                for (int ch = 0; ch < c.chunks[k]; ++ch) {
-                    const int4 x = __ldg(seg + ch);
-                    h += (1ull << (2 * occ5[x.x])) + (1ull << (2 * occ5[x.y])) + (1ull << (2 * occ5[x.z])) +
-                         (1ull << (2 * occ5[x.w]));
-                }
-            }
 #pragma unroll
             for (int i = 0; i < T; ++i)
-                if (a5 == 5 * i) acc[i][k] += h;
-            if (hist) hs[k] = pack_hist5<T>(h, c.pad[k]);
+                if (a5 == 5 * i) acc[i][k] += h[k];
+            if (hist) hs[k] = pack_hist5<T>(h[k], c.pad[k]);
         }
         if (hist) hist[s] = make_uint4(hs[0], hs[1], hs[2], (uint32_t)a5);
         if (++since == 32) {
             flush();
             since = 0;
+        }
+    };
+    if (c.lat.L) {  // implicit neighbours (no sentinel padding: pad[k] == 0)
+        lattice_sites<S, uint64_t>(c.lat, threadIdx.x, blockDim.x,
+                                   [occ5](int n) { return 1ull << (2 * occ5[n]); }, site);
+    } else {
+        for (int s = threadIdx.x; s < c.num_sites; s += blockDim.x) {
+            uint64_t h[S];
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                h[k] = 0;
+                const int4 *seg = nbor + (size_t)s * c.row4 + c.off4[k];
+                for (int ch = 0; ch < c.chunks[k]; ++ch) {
+                    const int4 x = __ldg(seg + ch);
+                    h[k] += (1ull << (2 * occ5[x.x])) + (1ull << (2 * occ5[x.y])) + (1ull << (2 * occ5[x.z])) +
+                            (1ull << (2 * occ5[x.w]));
+                }
+            }
+            site(s, h);
         }
     }
     flush();
