@@ -307,7 +307,7 @@ __global__ void nbmask_implicit_kernel(const SearchConst c, int row, uint32_t *m
     const int64_t total = (int64_t)c.num_sites * row;
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
         const int s = (int)(x / row), e = (int)(x % row);
-        const int n = lattice_neighbor(c.lat, site_pos(c.lat, s), e);
+        const int n = lattice_neighbor(c.lat, lattice_cell(c.lat, s), e);
         const uint32_t d = (uint32_t)(n - s + c.num_sites - 1);
         atomicOr(mask + (d >> 5), 1u << (d & 31u));
     }
@@ -526,19 +526,13 @@ void fill_lattice_const(const hea_problem *pb, SearchConst &c)
     LatticeConst &lc = c.lat;
     lc.L = pb->lattice_cell;
     lc.nb = sp.nb;
-    int e = 0;
-    for (int k = 0; k < 3; ++k) {
+    for (int k = 0, e = 0; k < 3; e += sp.size[k], ++k) {
         lc.zoff[k] = e;
         lc.zsize[k] = sp.size[k];
-        for (int v = 0; v < sp.size[k]; ++v, ++e)
-            for (int d = 0; d < 3; ++d) lc.vec[e][d] = (int8_t)sp.vec[k][v][d];
     }
-    for (int b = 0; b < 4; ++b)
-        for (int d = 0; d < 3; ++d) lc.basis[b][d] = (int8_t)(b < sp.nb ? sp.basis[b][d] : 0);
-    for (int q = 0; q < 8; ++q) lc.lut[q] = -1;
-    for (int b = 0; b < sp.nb; ++b)
-        lc.lut[((sp.basis[b][0] & 1) << 2) | ((sp.basis[b][1] & 1) << 1) | (sp.basis[b][2] & 1)] = (int8_t)b;
-    lc.kind = (int8_t)(pb->implicit_lattice == 2 ? kLatBcc : pb->lattice_shell_set == 1 ? kLatFccTrue3 : kLatFccRef);
+    lc.inv_L = 1.0 / lc.L;
+    lc.inv_LL = 1.0 / ((double)lc.L * lc.L);
+    lc.kind = pb->implicit_lattice == 2 ? kLatBcc : pb->lattice_shell_set == 1 ? kLatFccTrue3 : kLatFccRef;
     for (int k = 0; k < kMaxShells; ++k) c.pad[k] = 0;  // no sentinel padding in computed rows
 }
 
@@ -1686,7 +1680,7 @@ struct hea_batch {
         delete lv;
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
-        for (void *p : buffers) cudaFree(p);
+        for (void *p : buffers) dev_free(p);  // back to the block cache
         for (DeviceTables *t : tables) delete t;
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -1722,8 +1716,8 @@ __global__ void batch_reset_kernel(BatchCtl *ctl, BatchJob *jobs, unsigned long 
 template <class X>
 int batch_alloc(hea_batch *b, X **p, size_t bytes)
 {
-    void *q = nullptr;
-    if (cudaMalloc(&q, bytes) != cudaSuccess) return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes", bytes);
+    void *q = nullptr;  // from the block cache: a batch of the same shapes made again reuses the blocks
+    if (dev_alloc(&q, bytes) != cudaSuccess) return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes", bytes);
     b->buffers.push_back(q);
     *p = static_cast<X *>(q);
     return HEA_OK;

@@ -19,21 +19,21 @@
 namespace hea {
 
 // Implicit neighbour ids of a perfect FCC/BCC cube (the structure keeps no
-// neighbour table in memory).  Site s = nb (x L^2 + y L + z) + basis, position
-// in half lattice units 2 (x, y, z) + basis offset; the e-th neighbour of s
-// (shells concatenated) is the site at position(s) + vec[e], periodic in every
-// axis -- the same sites, in another order within each shell, as the table of
-// pyhea/lattice/lattice.py:196-323 (the order within a shell does not enter
-// any count or histogram).
+// neighbour table in memory).  Site s = nb (cx L^2 + cy L + cz) + b is basis
+// site b of cell (cx, cy, cz).  Its neighbours (shells concatenated) lie in
+// cells (cx + dx, cy + dy, cz + dz), d in {-1, 0, 1}, periodic in every axis,
+// at basis b' -- both fixed by the lattice's shell vectors.  Shell generators
+// in half lattice units: FCC (1,1,0) 12, (2,0,0) 6, then (2,2,0) 12 (reference
+// set) or (2,1,1) 24 (true third shell); BCC (1,1,1) 8, (2,0,0) 6, (2,2,0) 12.
+// The sets equal the table of pyhea/lattice/lattice.py:196-323; entries of a
+// shell come in another order, which no count or histogram sees.
 struct LatticeConst {
     int32_t L;                   // cube edge in cells; 0: the structure has a neighbour table
     int32_t nb;                  // basis sites per cell (4 FCC, 2 BCC)
-    int32_t zsize[3], zoff[3];   // shell sizes and their offsets into vec
-    int8_t basis[4][3];          // basis offsets, half units
-    int8_t vec[54][3];           // neighbour offsets, half units, shells concatenated
-    int8_t lut[8];               // basis index by position parity (x&1)*4 + (y&1)*2 + (z&1); -1: none
-    int8_t kind;                 // kLatFccRef, kLatFccTrue3 or kLatBcc (lattice_sites)
-    int8_t pad_;
+    int32_t zsize[3], zoff[3];   // shell sizes and offsets in the concatenated neighbour list
+    double inv_L, inv_LL;        // 1 / L and 1 / L^2, rounded (lattice_cell)
+    int32_t kind;                // kLatFccRef, kLatFccTrue3 or kLatBcc
+    int32_t pad_;
 };
 static_assert(sizeof(LatticeConst) % 8 == 0, "LatticeConst keeps SearchConst 8-byte sized");
 
@@ -52,48 +52,12 @@ struct SearchConst {
     LatticeConst lat;   // lat.L > 0: neighbours from lattice arithmetic (nbor unused)
 };
 
-struct SitePos {
-    int x, y, z;
-};
-
-// Position of site s in half lattice units.
-__device__ __forceinline__ SitePos site_pos(const LatticeConst &lc, int s)
-{
-    const int b = s & (lc.nb - 1), cell = s >> (lc.nb == 4 ? 2 : 1);  // nb is 2 or 4
-    const int LL = lc.L * lc.L, cx = cell / LL, r = cell - cx * LL, cy = r / lc.L, cz = r - cy * lc.L;
-    return SitePos{2 * cx + lc.basis[b][0], 2 * cy + lc.basis[b][1], 2 * cz + lc.basis[b][2]};
-}
-
-// The e-th neighbour (shells concatenated) of the site at position p.  Offsets
-// are at most 2 half units, so one wrap per axis keeps q in [0, 2L).
-__device__ __forceinline__ int lattice_neighbor(const LatticeConst &lc, const SitePos &p, int e)
-{
-    const int M = 2 * lc.L;
-    int qx = p.x + lc.vec[e][0], qy = p.y + lc.vec[e][1], qz = p.z + lc.vec[e][2];
-    qx += qx < 0 ? M : 0;
-    qy += qy < 0 ? M : 0;
-    qz += qz < 0 ? M : 0;
-    qx -= qx >= M ? M : 0;
-    qy -= qy >= M ? M : 0;
-    qz -= qz >= M ? M : 0;
-    const int bi = lc.lut[((qx & 1) << 2) | ((qy & 1) << 1) | (qz & 1)];
-    return lc.nb * (((qx >> 1) * lc.L + (qy >> 1)) * lc.L + (qz >> 1)) + bi;
-}
-
-// Compile-time geometry of the three implicit lattices, for the walks over
-// every site (recounts).  A neighbour of a site of basis b in cell (cx, cy, cz)
-// lies in cell (cx + dx, cy + dy, cz + dz), d in {-1, 0, 1}, at basis b'; with
-// (kind, b, shell, entry) known at compile time its id is one sum of three
-// per-site axis terms (LatticeAxes) and b'.  Shell generators in half units:
-// FCC (1,1,0) 12, (2,0,0) 6, then (2,2,0) 12 (reference set) or (2,1,1) 24
-// (true third shell); BCC (1,1,1) 8, (2,0,0) 6, (2,2,0) 12 -- the sets of
-// lattice_neighbor, entries in another order.
 enum : int { kLatFccRef = 0, kLatFccTrue3 = 1, kLatBcc = 2 };
 
 __host__ __device__ constexpr int lat_nb(int kind) { return kind == kLatBcc ? 2 : 4; }
 __host__ __device__ constexpr int lat_basis(int kind, int b, int d)
 {
-    // FCC {0,0,0} {1,1,0} {1,0,1} {0,1,1}; BCC {0,0,0} {1,1,1}
+    // half-unit basis offsets: FCC {0,0,0} {1,1,0} {1,0,1} {0,1,1}; BCC {0,0,0} {1,1,1}
     return kind == kLatBcc ? b : (b == 0 ? 0 : (d == 0 ? (b != 3) : d == 1 ? (b != 2) : (b != 1)));
 }
 __host__ __device__ constexpr int lat_gen(int kind, int k, int d)
@@ -106,34 +70,36 @@ __host__ __device__ constexpr int lat_shell_size(int kind, int k)
 {
     return k == 0 ? (kind == kLatBcc ? 8 : 12) : k == 1 ? 6 : (kind == kLatFccTrue3 ? 24 : 12);
 }
-// Component d of the i-th signed permutation of shell k's generator (48 candidates, duplicates included).
-__host__ __device__ constexpr int lat_candidate(int kind, int k, int i, int d)
+
+// The distinct signed axis permutations of shell k's generator, in a fixed order.
+struct LatVecs {
+    int n;
+    int v[24][3];
+};
+__host__ __device__ constexpr LatVecs lat_vecs(int kind, int k)
 {
+    LatVecs out{};
     const int perm[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
-    const int sgn = ((i >> (2 - d)) & 1) ? -1 : 1;  // i = 8 p + (sx sy sz)
-    return sgn * lat_gen(kind, k, perm[i >> 3][d]);
-}
-// Packed descriptor of entry e of shell k for basis b: (dx+1) | (dy+1) << 2 | (dz+1) << 4 | b' << 6.
-__host__ __device__ constexpr int lat_desc(int kind, int b, int k, int e)
-{
-    int seen = -1, pick = 0;
-    for (int i = 0; i < 48 && seen < e; ++i) {
+    for (int i = 0; i < 48; ++i) {
+        int c[3] = {0, 0, 0};
+        for (int d = 0; d < 3; ++d) c[d] = (((i >> (2 - d)) & 1) ? -1 : 1) * lat_gen(kind, k, perm[i >> 3][d]);
         bool dup = false;
-        for (int j = 0; j < i && !dup; ++j)
-            dup = lat_candidate(kind, k, j, 0) == lat_candidate(kind, k, i, 0) &&
-                  lat_candidate(kind, k, j, 1) == lat_candidate(kind, k, i, 1) &&
-                  lat_candidate(kind, k, j, 2) == lat_candidate(kind, k, i, 2);
+        for (int j = 0; j < out.n && !dup; ++j) dup = out.v[j][0] == c[0] && out.v[j][1] == c[1] && out.v[j][2] == c[2];
         if (!dup) {
-            ++seen;
-            pick = i;
+            for (int d = 0; d < 3; ++d) out.v[out.n][d] = c[d];
+            ++out.n;
         }
     }
+    return out;
+}
+// Packed neighbour descriptor for basis b and offset v: (dx+1) | (dy+1) << 2 | (dz+1) << 4 | b' << 6.
+__host__ __device__ constexpr int lat_pack(int kind, int b, const int (&v)[3])
+{
     int out = 0, par[3] = {0, 0, 0};
     for (int d = 0; d < 3; ++d) {
-        const int q = lat_basis(kind, b, d) + lat_candidate(kind, k, pick, d);  // -2 .. 3
-        const int cell = q >= 0 ? q / 2 : -1;
+        const int q = lat_basis(kind, b, d) + v[d];  // -2 .. 3 half units
         par[d] = q & 1;
-        out |= (cell + 1) << (2 * d);
+        out |= ((q >= 0 ? q / 2 : -1) + 1) << (2 * d);
     }
     int bp = 0;
     for (int x = 0; x < lat_nb(kind); ++x)
@@ -141,7 +107,98 @@ __host__ __device__ constexpr int lat_desc(int kind, int b, int k, int e)
             bp = x;
     return out | (bp << 6);
 }
+__host__ __device__ constexpr int lat_desc(int kind, int b, int k, int e) { return lat_pack(kind, b, lat_vecs(kind, k).v[e]); }
 
+// Every descriptor, shells concatenated, for the per-lane lookups of
+// lattice_neighbor (a global table: lanes read different entries, which the
+// constant bank would serialise).
+struct LatDescTable {
+    uint8_t d[3][4][54];
+};
+__host__ __device__ constexpr LatDescTable make_lat_desc_table()
+{
+    LatDescTable t{};
+    for (int kind = 0; kind < 3; ++kind) {
+        int e0 = 0;
+        for (int k = 0; k < 3; ++k) {
+            const LatVecs vs = lat_vecs(kind, k);
+            for (int b = 0; b < lat_nb(kind); ++b)
+                for (int e = 0; e < vs.n; ++e) t.d[kind][b][e0 + e] = (uint8_t)lat_pack(kind, b, vs.v[e]);
+            e0 += vs.n;
+        }
+    }
+    return t;
+}
+__device__ const LatDescTable kLatDesc = make_lat_desc_table();
+
+// floor(n / d) for 0 <= n < 2^31, d <= 2^20, from inv = 1/d rounded: n * inv is
+// within 2^-21 of n / d, so the truncation is the quotient or one less, and
+// one correction makes it exact.
+__device__ __forceinline__ int div_by(int n, int d, double inv)
+{
+    int q = __double2int_rz(__dmul_rn((double)n, inv));
+    q += (n - q * d) >= d;
+    return q;
+}
+
+struct LatticeCell {
+    int b, x, y, z;
+};
+
+__device__ __forceinline__ LatticeCell lattice_cell(const LatticeConst &lc, int s)
+{
+    const int cell = s >> (lc.nb == 4 ? 2 : 1), LL = lc.L * lc.L;  // nb is 2 or 4
+    const int x = div_by(cell, LL, lc.inv_LL), r = cell - x * LL, y = div_by(r, lc.L, lc.inv_L);
+    return LatticeCell{s & (lc.nb - 1), x, y, r - y * lc.L};
+}
+
+// Entry e (shells concatenated) of the neighbour list of the site in cell p.
+__device__ __forceinline__ int lattice_neighbor(const LatticeConst &lc, const LatticeCell &p, int e)
+{
+    const int d = __ldg(&kLatDesc.d[lc.kind][p.b][e]), L = lc.L;
+    int x = p.x + (d & 3) - 1, y = p.y + ((d >> 2) & 3) - 1, z = p.z + ((d >> 4) & 3) - 1;
+    x += x < 0 ? L : 0;
+    y += y < 0 ? L : 0;
+    z += z < 0 ? L : 0;
+    x -= x >= L ? L : 0;
+    y -= y >= L ? L : 0;
+    z -= z >= L ? L : 0;
+    return lc.nb * ((x * L + y) * L + z) + (d >> 6);
+}
+
+// How often s2 is listed in each of the first S shells of s1's neighbour
+// list, in closed form: the displacement from s1 to s2 in half units, wrapped
+// to (-L, L] per axis, is a shell vector iff its absolute components form the
+// shell's pattern (FCC 1,1,0 | 2,0,0 | 2,2,0 or 2,1,1; BCC 1,1,1 | 2,0,0 |
+// 2,2,0).  At L = 2 the vectors +2 and -2 along an axis reach the same site,
+// so each such component doubles the count.  s1 != s2.
+template <int S>
+__device__ __forceinline__ void lattice_multiplicity(const LatticeConst &lc, int s1, int s2, uint32_t (&m)[S])
+{
+    const LatticeCell p = lattice_cell(lc, s1), q = lattice_cell(lc, s2);
+    const int M = 2 * lc.L, pc[3] = {p.x, p.y, p.z}, qc[3] = {q.x, q.y, q.z};
+    int n0 = 0, n1 = 0, n2 = 0, mult = 1;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        int v = 2 * (qc[d] - pc[d]) + lat_basis(lc.kind, q.b, d) - lat_basis(lc.kind, p.b, d);  // (-2L, 2L)
+        v -= v > lc.L ? M : 0;
+        v += v <= -lc.L ? M : 0;
+        const int a = v < 0 ? -v : v;
+        n0 += a == 0;
+        n1 += a == 1;
+        n2 += a == 2;
+        mult <<= (M == 4 && a == 2) ? 1 : 0;
+    }
+    const bool bcc = lc.kind == kLatBcc, true3 = lc.kind == kLatFccTrue3;
+    const bool in[3] = {bcc ? n1 == 3 : (n1 == 2 && n0 == 1), n2 == 1 && n0 == 2,
+                        true3 ? (n2 == 1 && n1 == 2) : (n2 == 2 && n0 == 1)};
+#pragma unroll
+    for (int k = 0; k < S; ++k) m[k] = in[k] ? (uint32_t)mult : 0u;
+}
+
+// Compile-time form of the same geometry for the walks over every site
+// (recounts): with (kind, b, shell, entry) known at compile time a
+// neighbour's id is one sum of three per-site axis terms (LatticeAxes) and b'.
 // Per-site axis terms: x[d] = nb L^2 wrap(cx + d - 1), y[d] = nb L wrap(cy + d - 1), z[d] = nb wrap(cz + d - 1).
 struct LatticeAxes {
     int x[3], y[3], z[3];
@@ -435,13 +492,12 @@ __device__ __forceinline__ double score_delta(const SearchConst &c, const int4 *
     const int a5 = 5 * a, b5 = 5 * b;
     if (near) {
         if (c.lat.L) {  // implicit neighbours
-            const SitePos p1 = site_pos(c.lat, (int)s1);
+            uint32_t m[S];
+            lattice_multiplicity<S>(c.lat, (int)s1, (int)s2, m);
 #pragma unroll
             for (int k = 0; k < S; ++k) {
-                uint32_t m = 0;
-                for (int v = 0; v < c.lat.zsize[k]; ++v) m += lattice_neighbor(c.lat, p1, c.lat.zoff[k] + v) == (int)s2;
-                h1[k] += m << a5;
-                h2[k] += m << b5;
+                h1[k] += m[k] << a5;
+                h2[k] += m[k] << b5;
             }
         } else {
             const int row4 = L::kRuntime ? c.row4 : L::kRow4;
@@ -492,7 +548,7 @@ __device__ __forceinline__ void update_hist(const SearchConst &c, const int4 *__
         for (int e = me; e < 2 * row; e += blockDim.x) {
             const bool first = e < row;
             const int idx = first ? e : e - row;
-            const int n = lattice_neighbor(c.lat, site_pos(c.lat, (int)(first ? s1 : s2)), idx);
+            const int n = lattice_neighbor(c.lat, lattice_cell(c.lat, (int)(first ? s1 : s2)), idx);
             int k = 0;
 #pragma unroll
             for (int kk = 1; kk < L::S; ++kk) k += idx >= c.lat.zoff[kk];
