@@ -76,17 +76,17 @@ HBM_FALLBACK_GBS = 6650.0
 #   inst   smsp__inst_executed.sum (warp instructions)        -> roofline.issue_frac
 #   dram_read  dram__bytes_read.sum                           -> roofline.dram_random (batched)
 # mc_kernel<5, Shells<2,2,3>>: the first local-search launch of `python bench.py --case plain
-# --iters 1` (203.72 M evaluations): 71.68 MB + 93.46 MB DRAM, 437.14 M L2 sectors, 3.9646 G warp
+# --iters 1` (203.72 M evaluations): 71.73 MB + 92.58 MB DRAM, 435.41 M L2 sectors, 4.1029 G warp
 # instructions.  batch_kernel: the launch of `python bench.py --case batch --count 64 --iters 10`, the
-# bench's batch configuration (6268.46 M evaluations): 1342.0 GB + 73.23 GB DRAM, 83.37 G L2 sectors,
-# 181.29 G warp instructions.  dram_random_probe_kernel (hea_dram_random_probe over 4 GiB, 77.59 M
+# bench's batch configuration (6268.46 M evaluations): 1302.02 GB + 68.62 GB DRAM, 77.165 G L2 sectors,
+# 179.15 G warp instructions.  dram_random_probe_kernel (hea_dram_random_probe over 4 GiB, 77.59 M
 # random 16-byte loads): 9.833 GB DRAM read, i.e. 126.7 B per load (each load fetches a 128-byte line).
 KERNEL_COUNTERS = {
-    "plain_gpu": {"dram": (71.68e6 + 93.46e6) / 203.72e6, "l2": 437.14e6 * 32.0 / 203.72e6,
-                  "inst": 3.9646e9 / 203.72e6,
+    "plain_gpu": {"dram": (71.73e6 + 92.58e6) / 203.72e6, "l2": 435.41e6 * 32.0 / 203.72e6,
+                  "inst": 4.1029e9 / 203.72e6,
                   "capture": "mc_kernel, first local-search launch of bench.py --case plain --iters 1"},
-    "batched": {"dram": (1342.0e9 + 73.23e9) / 6268.46e6, "l2": 83.37e9 * 32.0 / 6268.46e6,
-                "inst": 181.29e9 / 6268.46e6, "dram_read": 1342.0e9 / 6268.46e6,
+    "batched": {"dram": (1302.02e9 + 68.62e9) / 6268.46e6, "l2": 77.165e9 * 32.0 / 6268.46e6,
+                "inst": 179.15e9 / 6268.46e6, "dram_read": 1302.02e9 / 6268.46e6,
                 "capture": "batch_kernel, bench.py --case batch --count 64 --iters 10"},
 }
 DRAM_BYTES_PER_RANDOM_LOAD = 9.833e9 / 77.594624e6
@@ -387,11 +387,43 @@ def measure_batched(steps, warmup, l2_peak=None, implicit=False):
         t0 = time.perf_counter()
         eb = hb.Batch(pinned, params)
         s = eb.run(seeds(warmup + k))
-        for i in range(len(structs)):
-            eb.read(i)
+        last = [eb.read(i)[0] for i in range(len(structs))]
         eb.close()
         e2e_s += time.perf_counter() - t0
         e2e_ev += s["evals"]
+
+    # the same structures described by their lattices (no neighbour tables): device and end-to-end
+    # rates, and the results of the last step compared with the tables'
+    implicit_block = None
+    if not implicit:
+        ip = [pinned_problem(st.problem(implicit=True)) for st in structs]
+        ib = hb.Batch(ip, params)
+        ib.run(seeds(0))
+        i_ms = i_ev = 0
+        for k in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            s = ib.run(seeds(warmup + k))
+            i_ms += s["gpu_ms"]
+            i_ev += s["evals"]
+        ib.close()
+        ie_s, ie_ev = 0.0, 0
+        for k in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eb = hb.Batch(ip, params)
+            s = eb.run(seeds(warmup + k))
+            got = [eb.read(i)[0] for i in range(len(structs))]
+            eb.close()
+            ie_s += time.perf_counter() - t0
+            ie_ev += s["evals"]
+        isame = sum(int(np.array_equal(a, b)) for a, b in zip(got, last))
+        implicit_block = {"value": i_ev / (i_ms / 1000.0), "unit": "swap-evals/s", "ms_per_step": i_ms / steps,
+                          "identical_structures": isame,
+                          "e2e": {"value": ie_ev / ie_s, "unit": "swap-evals/s",
+                                  "h2d_bytes_per_step": int(sum(problem_bytes(pb) for pb in ip)),
+                                  "d2h_bytes_per_step": int(d2h)}}
 
     # roofline: each structure's algorithmic bytes per evaluation (BCC 8/6/12 262 B, FCC 12/6/24
     # 422 B) weighted by its evaluations in the last step
@@ -413,12 +445,14 @@ def measure_batched(steps, warmup, l2_peak=None, implicit=False):
             "config": {"workload": "batched: 64 mixed FCC/BCC structures",
                        "sites_total": int(sum(st.num_sites for st in structs)), "solutions": 64,
                        "parallel_task": 256, "total_iter": 10, "converge_depth": 10,
-                       "l2": "flushed between timed steps (256 MiB write)", "batch_launch": tuned},
+                       "l2": "flushed between timed steps (256 MiB write)", "batch_launch": tuned,
+                       "neighbours": "implicit (lattice arithmetic, no table)" if implicit else "table"},
             "plain": {"value": plain, "ms_per_step": p_ms / steps, "evals_per_step": p_ev / steps},
             "speedup_vs_plain": value / plain, "identical_structures": same, "structures": len(structs),
             "evals_per_step": b_ev / steps, "clocks": clocks, "roofline": roof,
             "e2e": {"value": e2e_ev / e2e_s, "unit": "swap-evals/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
+            **({"implicit_neighbours": implicit_block} if implicit_block else {}),
             # one CUDA graph per step: queue reset, phase-0 seeding, the persistent kernel
             "gpu_launches": 3 * steps}
 
