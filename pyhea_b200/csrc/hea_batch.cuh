@@ -61,7 +61,9 @@ struct BatchJob {
 static_assert(sizeof(BatchJob) == 32, "BatchJob layout");
 
 // Kernel instance of a structure: species count and shell layout.
-enum BatchLayout : int32_t { kLayBcc = 0, kLayFccTrue = 1, kLayRt1 = 2, kLayRt2 = 3, kLayRt3 = 4 };
+enum BatchLayout : int32_t {
+    kLayBcc = 0, kLayFccTrue = 1, kLayRt1 = 2, kLayRt2 = 3, kLayRt3 = 4, kLayImp1 = 5, kLayImp2 = 6, kLayImp3 = 7
+};
 
 struct BatchStruct {
     SearchConst c;
@@ -314,6 +316,9 @@ __device__ __forceinline__ JobEnd batch_dispatch_t(const SearchConst &c, const B
     case kLayFccTrue: return batch_job<T, Shells<3, 2, 6>>(c, d, job, smem, stats, tally, deadline);
     case kLayRt1: return batch_job<T, RuntimeShells<1>>(c, d, job, smem, stats, tally, deadline);
     case kLayRt2: return batch_job<T, RuntimeShells<2>>(c, d, job, smem, stats, tally, deadline);
+    case kLayImp1: return batch_job<T, ImplicitShells<1>>(c, d, job, smem, stats, tally, deadline);
+    case kLayImp2: return batch_job<T, ImplicitShells<2>>(c, d, job, smem, stats, tally, deadline);
+    case kLayImp3: return batch_job<T, ImplicitShells<3>>(c, d, job, smem, stats, tally, deadline);
     default: return batch_job<T, RuntimeShells<3>>(c, d, job, smem, stats, tally, deadline);
     }
 }

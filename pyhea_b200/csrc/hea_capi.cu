@@ -168,8 +168,10 @@ const GenFn kGen[kMaxTypes + 1][kMaxShells + 1] = {
 // the layouts of the FCC/BCC shell sets (in int4 chunks per shell) have their
 // loads unrolled; any other table uses the runtime-layout instance.
 template <int T>
-McFn pick_mc_t(int c0, int c1, int c2, int S)
+McFn pick_mc_t(int c0, int c1, int c2, int S, bool implicit)
 {
+    if (implicit) return S == 1 ? mc_kernel<T, ImplicitShells<1>> : S == 2 ? mc_kernel<T, ImplicitShells<2>>
+                                                                          : mc_kernel<T, ImplicitShells<3>>;
     if (c0 == 2 && c1 == 0 && c2 == 0) return mc_kernel<T, Shells<2, 0, 0>>;  // BCC, 1 shell
     if (c0 == 2 && c1 == 2 && c2 == 0) return mc_kernel<T, Shells<2, 2, 0>>;  // BCC, 2 shells
     if (c0 == 2 && c1 == 2 && c2 == 3) return mc_kernel<T, Shells<2, 2, 3>>;  // BCC 8/6/12
@@ -184,8 +186,11 @@ McFn pick_mc_t(int c0, int c1, int c2, int S)
 
 // The same choice for the HBM-occupancy (cluster) search.
 template <int T>
-McFn pick_mc_large_t(int c0, int c1, int c2, int S)
+McFn pick_mc_large_t(int c0, int c1, int c2, int S, bool implicit)
 {
+    if (implicit)
+        return S == 1 ? mc_large_kernel<T, ImplicitShells<1>>
+                      : S == 2 ? mc_large_kernel<T, ImplicitShells<2>> : mc_large_kernel<T, ImplicitShells<3>>;
     if (c0 == 2 && c1 == 2 && c2 == 3) return mc_large_kernel<T, Shells<2, 2, 3>>;
     if (c0 == 3 && c1 == 2 && c2 == 3) return mc_large_kernel<T, Shells<3, 2, 3>>;
     if (c0 == 3 && c1 == 2 && c2 == 6) return mc_large_kernel<T, Shells<3, 2, 6>>;
@@ -194,14 +199,14 @@ McFn pick_mc_large_t(int c0, int c1, int c2, int S)
     return mc_large_kernel<T, RuntimeShells<3>>;
 }
 
-McFn pick_mc_large(int T, int c0, int c1, int c2, int S)
+McFn pick_mc_large(int T, int c0, int c1, int c2, int S, bool implicit)
 {
     switch (T) {
-    case 2: return pick_mc_large_t<2>(c0, c1, c2, S);
-    case 3: return pick_mc_large_t<3>(c0, c1, c2, S);
-    case 4: return pick_mc_large_t<4>(c0, c1, c2, S);
-    case 5: return pick_mc_large_t<5>(c0, c1, c2, S);
-    default: return pick_mc_large_t<6>(c0, c1, c2, S);
+    case 2: return pick_mc_large_t<2>(c0, c1, c2, S, implicit);
+    case 3: return pick_mc_large_t<3>(c0, c1, c2, S, implicit);
+    case 4: return pick_mc_large_t<4>(c0, c1, c2, S, implicit);
+    case 5: return pick_mc_large_t<5>(c0, c1, c2, S, implicit);
+    default: return pick_mc_large_t<6>(c0, c1, c2, S, implicit);
     }
 }
 
@@ -227,14 +232,14 @@ __global__ void zero_counts_kernel(const int32_t *order, int count, int32_t *cnt
     for (int x = threadIdx.x; x < ncount; x += blockDim.x) g[x] = 0;
 }
 
-McFn pick_mc(int T, int c0, int c1, int c2, int S)
+McFn pick_mc(int T, int c0, int c1, int c2, int S, bool implicit)
 {
     switch (T) {
-    case 2: return pick_mc_t<2>(c0, c1, c2, S);
-    case 3: return pick_mc_t<3>(c0, c1, c2, S);
-    case 4: return pick_mc_t<4>(c0, c1, c2, S);
-    case 5: return pick_mc_t<5>(c0, c1, c2, S);
-    default: return pick_mc_t<6>(c0, c1, c2, S);
+    case 2: return pick_mc_t<2>(c0, c1, c2, S, implicit);
+    case 3: return pick_mc_t<3>(c0, c1, c2, S, implicit);
+    case 4: return pick_mc_t<4>(c0, c1, c2, S, implicit);
+    case 5: return pick_mc_t<5>(c0, c1, c2, S, implicit);
+    default: return pick_mc_t<6>(c0, c1, c2, S, implicit);
     }
 }
 
@@ -632,6 +637,21 @@ void fill_const(const hea_problem *pb, uint64_t seed, SearchConst &c, PadGeom &g
     fill_lattice_const(pb, c);
 }
 
+// Histogram bytes above which a structure streams its histogram loads
+// (SearchConst::hist_stream): a plan, whose structure has the L2 to itself,
+// from twice the L2 size; a batch or server structure, which shares L2 with
+// the others, from kSharedStreamBytes.
+constexpr size_t kSharedStreamBytes = (size_t)64 << 20;  // measured on the mixed batch: 4, 16, 64 MiB within 0.4 %
+
+uint32_t stream_histograms(size_t hist_bytes, bool shared)
+{
+    if (shared) return hist_bytes > kSharedStreamBytes ? 1u : 0u;
+    int dev = 0, l2 = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
+    return hist_bytes > 2 * (size_t)l2 ? 1u : 0u;
+}
+
 int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t flags = 0)
 {
     HEA_TRY(validate_problem(pb));
@@ -652,14 +672,14 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t
     if (dt.smem_mc > (size_t)smem_limit() || (flags & HEA_FLAG_HBM_OCCUPANCY)) {
         // structures beyond shared memory: occupancy in HBM, cluster search
         dt.large = true;
-        dt.mc = pick_mc_large(T, c.chunks[0], S > 1 ? c.chunks[1] : 0, S > 2 ? c.chunks[2] : 0, S);
+        dt.mc = pick_mc_large(T, c.chunks[0], S > 1 ? c.chunks[1] : 0, S > 2 ? c.chunks[2] : 0, S, c.lat.L > 0);
         dt.lgen = kLGen[T];
         dt.lrec = kLRec[T][S];
         dt.lfit = kLFit[T][S];
         HEA_CUDA(allow_max_smem(dt.mc));
     } else {
         dt.gen = kGen[T][S];
-        dt.mc = pick_mc(T, c.chunks[0], S > 1 ? c.chunks[1] : 0, S > 2 ? c.chunks[2] : 0, S);
+        dt.mc = pick_mc(T, c.chunks[0], S > 1 ? c.chunks[1] : 0, S > 2 ? c.chunks[2] : 0, S, c.lat.L > 0);
         HEA_CUDA(allow_max_smem(dt.gen));
         HEA_CUDA(allow_max_smem(dt.mc));
     }
@@ -1124,6 +1144,7 @@ int plan_create(const hea_problem *pb, const hea_params *prm, int slots, hea_pla
         pl->P = prm->num_solutions;
         pl->mc_block = choose_block(prm->parallel_task);
         rc = plan_alloc(pl, slots);
+        pl->dt.c.hist_stream = stream_histograms((size_t)slots * pl->dt.N * sizeof(uint4), false);
     }
     if (rc == HEA_OK) rc = plan_autotune(pl, (prm->flags & HEA_FLAG_AUTOTUNE) != 0);
     if (rc != HEA_OK) {
@@ -1725,6 +1746,7 @@ int batch_alloc(hea_batch *b, X **p, size_t bytes)
 
 int batch_layout(const SearchConst &c, int S)
 {
+    if (c.lat.L) return S == 1 ? kLayImp1 : (S == 2 ? kLayImp2 : kLayImp3);
     if (S == 3 && c.chunks[0] == 2 && c.chunks[1] == 2 && c.chunks[2] == 3) return kLayBcc;
     if (S == 3 && c.chunks[0] == 3 && c.chunks[1] == 2 && c.chunks[2] == 6) return kLayFccTrue;
     return S == 1 ? kLayRt1 : (S == 2 ? kLayRt2 : kLayRt3);
@@ -1833,6 +1855,7 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
         const int P = params[i].num_solutions, slots = 2 * P;
         BatchStruct d{};
         d.c = t->c;
+        d.c.hist_stream = stream_histograms((size_t)slots * t->N * sizeof(uint4), true);
         d.nbor = t->nbor;
         d.P = P;
         d.Q = params[i].parallel_task;
@@ -2300,6 +2323,7 @@ int server_place(hea_server *sv, ServerRequest &r, int slot)
     }
     BatchStruct d{};
     d.c = c;
+    d.c.hist_stream = stream_histograms((size_t)2 * P * r.N * sizeof(uint4), true);
     d.nbor = implicit ? nullptr : reinterpret_cast<const int4 *>(base + L.nbor);
     d.occ = base + L.occ;
     d.cnt = reinterpret_cast<int32_t *>(base + L.cnt);
