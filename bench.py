@@ -76,17 +76,17 @@ HBM_FALLBACK_GBS = 6650.0
 #   inst   smsp__inst_executed.sum (warp instructions)        -> roofline.issue_frac
 #   dram_read  dram__bytes_read.sum                           -> roofline.dram_random (batched)
 # mc_kernel<5, Shells<2,2,3>>: the first local-search launch of `python bench.py --case plain
-# --iters 1` (203.72 M evaluations): 71.73 MB + 92.58 MB DRAM, 435.41 M L2 sectors, 4.1029 G warp
+# --iters 1` (203.72 M evaluations): 72.86 MB + 92.45 MB DRAM, 434.05 M L2 sectors, 4.0537 G warp
 # instructions.  batch_kernel: the launch of `python bench.py --case batch --count 64 --iters 10`, the
-# bench's batch configuration (6268.46 M evaluations): 1302.02 GB + 68.62 GB DRAM, 77.165 G L2 sectors,
-# 179.15 G warp instructions.  dram_random_probe_kernel (hea_dram_random_probe over 4 GiB, 77.59 M
+# bench's batch configuration (6268.46 M evaluations): 1192.25 GB + 63.38 GB DRAM, 75.461 G L2 sectors,
+# 177.27 G warp instructions.  dram_random_probe_kernel (hea_dram_random_probe over 4 GiB, 77.59 M
 # random 16-byte loads): 9.833 GB DRAM read, i.e. 126.7 B per load (each load fetches a 128-byte line).
 KERNEL_COUNTERS = {
-    "plain_gpu": {"dram": (71.73e6 + 92.58e6) / 203.72e6, "l2": 435.41e6 * 32.0 / 203.72e6,
-                  "inst": 4.1029e9 / 203.72e6,
+    "plain_gpu": {"dram": (72.86e6 + 92.45e6) / 203.72e6, "l2": 434.05e6 * 32.0 / 203.72e6,
+                  "inst": 4.0537e9 / 203.72e6,
                   "capture": "mc_kernel, first local-search launch of bench.py --case plain --iters 1"},
-    "batched": {"dram": (1302.02e9 + 68.62e9) / 6268.46e6, "l2": 77.165e9 * 32.0 / 6268.46e6,
-                "inst": 179.15e9 / 6268.46e6, "dram_read": 1302.02e9 / 6268.46e6,
+    "batched": {"dram": (1192.25e9 + 63.38e9) / 6268.46e6, "l2": 75.461e9 * 32.0 / 6268.46e6,
+                "inst": 177.27e9 / 6268.46e6, "dram_read": 1192.25e9 / 6268.46e6,
                 "capture": "batch_kernel, bench.py --case batch --count 64 --iters 10"},
 }
 DRAM_BYTES_PER_RANDOM_LOAD = 9.833e9 / 77.594624e6

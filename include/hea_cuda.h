@@ -108,10 +108,11 @@ void hea_release_cached_memory(void);
 int hea_l2_read_probe(int64_t bytes, int32_t reps, double *out_gbs);
 
 /* Random 16-byte loads per second from a buffer of `bytes` (far larger than
- * L2), each through L2 only, per_thread loads by each of 8 CTAs x 256 threads
- * per SM after one warm-up launch: the ceiling of the site-histogram loads of
- * structures whose histograms stay in DRAM (each load moves a 32-byte sector).
- * A measurement aid with no counterpart in the reference. */
+ * L2), per_thread loads by each thread of 8 and of 32 CTAs x 256 threads per
+ * SM, L2-cached and evict-first, each after one warm-up launch; the best rate:
+ * the ceiling of the site-histogram loads of structures whose histograms stay
+ * in DRAM (each such load brings a 128-byte line from DRAM on B200).  A
+ * measurement aid with no counterpart in the reference. */
 int hea_dram_random_probe(int64_t bytes, int32_t per_thread, double *out_loads_per_s);
 
 /*

@@ -545,7 +545,8 @@ def l2_read_probe(nbytes=32 << 20, reps=50):
 
 
 def dram_random_probe(nbytes=4 << 30, per_thread=256):
-    """hea_dram_random_probe: random 16-byte loads per second from a buffer of `nbytes` in DRAM."""
+    """hea_dram_random_probe: random 16-byte loads per second from a buffer of `nbytes` in DRAM
+    (the best of L2-cached and evict-first loads at 8 and 32 CTAs per SM)."""
     out = _f64()
     _check(_load().hea_dram_random_probe(int(nbytes), int(per_thread), ctypes.byref(out)))
     return out.value
