@@ -637,19 +637,22 @@ void fill_const(const hea_problem *pb, uint64_t seed, SearchConst &c, PadGeom &g
     fill_lattice_const(pb, c);
 }
 
-// Histogram bytes above which a structure streams its histogram loads
-// (SearchConst::hist_stream): a plan, whose structure has the L2 to itself,
-// from twice the L2 size; a batch or server structure, which shares L2 with
-// the others, from kSharedStreamBytes.
-constexpr size_t kSharedStreamBytes = (size_t)64 << 20;  // measured on the mixed batch: 4, 16, 64 MiB within 0.4 %
+// Whether a structure streams its histogram loads (SearchConst::hist_stream).
+// `total_bytes` is the histogram memory of every structure resident with it
+// (its own alone for a plan).  Until that total passes twice the L2 size the
+// structures keep their lines cached; beyond it, those with more than
+// kSharedStreamBytes of their own stream, so that the lines of the smaller
+// ones stay.  Measured: a single 131 MB structure loses 3 % by streaming; on
+// the mixed batch (3.7 GB) thresholds of 4, 16 and 64 MiB are within 0.4 %.
+constexpr size_t kSharedStreamBytes = (size_t)64 << 20;
 
-uint32_t stream_histograms(size_t hist_bytes, bool shared)
+uint32_t stream_histograms(size_t hist_bytes, size_t total_bytes)
 {
-    if (shared) return hist_bytes > kSharedStreamBytes ? 1u : 0u;
     int dev = 0, l2 = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev);
-    return hist_bytes > 2 * (size_t)l2 ? 1u : 0u;
+    if (total_bytes <= 2 * (size_t)l2) return 0u;
+    return hist_bytes > kSharedStreamBytes ? 1u : 0u;
 }
 
 int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t flags = 0)
@@ -1144,7 +1147,8 @@ int plan_create(const hea_problem *pb, const hea_params *prm, int slots, hea_pla
         pl->P = prm->num_solutions;
         pl->mc_block = choose_block(prm->parallel_task);
         rc = plan_alloc(pl, slots);
-        pl->dt.c.hist_stream = stream_histograms((size_t)slots * pl->dt.N * sizeof(uint4), false);
+        const size_t hist_bytes = (size_t)slots * pl->dt.N * sizeof(uint4);
+        pl->dt.c.hist_stream = stream_histograms(hist_bytes, hist_bytes);
     }
     if (rc == HEA_OK) rc = plan_autotune(pl, (prm->flags & HEA_FLAG_AUTOTUNE) != 0);
     if (rc != HEA_OK) {
@@ -1846,6 +1850,10 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
     hea_batch *b = new (std::nothrow) hea_batch();
     if (!b) return fail(HEA_ERR_NOMEM, "out of host memory");
     b->count = count;
+    size_t hist_total = 0;  // site-histogram bytes of all structures (stream_histograms)
+    for (int i = 0; i < count; ++i)
+        hist_total += (size_t)2 * std::max(0, params[i].num_solutions) * std::max(0, problems[i].num_sites) *
+                      sizeof(uint4);
     int rc = HEA_OK;
     for (int i = 0; i < count && rc == HEA_OK; ++i) {
         rc = validate_params(&params[i]);
@@ -1865,7 +1873,7 @@ int hea_batch_create(const hea_problem *problems, const hea_params *params, int3
         const int P = params[i].num_solutions, slots = 2 * P;
         BatchStruct d{};
         d.c = t->c;
-        d.c.hist_stream = stream_histograms((size_t)slots * t->N * sizeof(uint4), true);
+        d.c.hist_stream = stream_histograms((size_t)slots * t->N * sizeof(uint4), hist_total);
         d.nbor = t->nbor;
         d.P = P;
         d.Q = params[i].parallel_task;
@@ -2124,6 +2132,7 @@ struct ServerRequest {
     int lattice = -1, cell = 0, shell_set = 0;
     int slot = -1, hbm = 0;
     size_t off = 0, bytes = 0;
+    size_t hist_bytes = 0;  // site-histogram bytes of the placed request
     double t_submit = 0, t_admit = 0, t_finish = 0, device_ms = 0;
     int iterations = 0;
     unsigned long long tally[3] = {0, 0, 0};
@@ -2198,6 +2207,7 @@ struct hea_server {
     std::vector<void *> buffers;
     uint8_t *arena = nullptr;
     ArenaHeap heap;
+    size_t hist_placed = 0;  // site-histogram bytes of the placed requests (stream_histograms)
     BatchStruct *d_structs = nullptr;
     BatchState *d_states = nullptr;
     BatchJob *d_jobs = nullptr;
@@ -2333,7 +2343,9 @@ int server_place(hea_server *sv, ServerRequest &r, int slot)
     }
     BatchStruct d{};
     d.c = c;
-    d.c.hist_stream = stream_histograms((size_t)2 * P * r.N * sizeof(uint4), true);
+    r.hist_bytes = (size_t)2 * P * r.N * sizeof(uint4);
+    sv->hist_placed += r.hist_bytes;
+    d.c.hist_stream = stream_histograms(r.hist_bytes, sv->hist_placed);
     d.nbor = implicit ? nullptr : reinterpret_cast<const int4 *>(base + L.nbor);
     d.occ = base + L.occ;
     d.cnt = reinterpret_cast<int32_t *>(base + L.cnt);
@@ -2366,6 +2378,7 @@ void server_release(hea_server *sv, ServerRequest &r)
 {
     if (r.slot < 0) return;
     sv->heap.release(r.off, r.bytes);
+    sv->hist_placed -= r.hist_bytes;
     sv->level_load[r.level] -= 2ull * r.params.num_solutions;
     sv->slot_req[r.slot] = 0;
     r.slot = -1;
