@@ -117,3 +117,27 @@ def test_autotuned_batch_gives_the_same_results():
         np.testing.assert_array_equal(occ, pocc, err_msg=f"structure {i}")
         np.testing.assert_array_equal(fit, pfit, err_msg=f"structure {i}")
     b.close()
+
+
+def test_streaming_histogram_loads_give_the_same_results():
+    """Two FCC 30^3 structures (108 000 sites, 64 solutions): 221 MB of site histograms each, 442 MB
+    together, more than twice the L2, so the batch reads both with evict-first loads; searched alone
+    each fits the plain path's cached policy.  The load policy must not change a result."""
+    rng = np.random.default_rng(5)
+    items = []
+    for i, implicit in enumerate((False, True)):
+        n = L.num_sites(L.FCC, 30)
+        species = W.dirichlet_counts(rng, 4, n)
+        st = W.small_case(lattice=L.FCC, cell=30, species=species, shells=3, shell_set=L.SHELLS_FCC_TRUE3, seed=40 + i)
+        items.append(st.problem(device=True, implicit=implicit))
+    q = dict(num_solutions=64, total_iter=1, parallel_task=64, converge_depth=3)
+    seeds = [71, 72]
+    b = hb.Batch(items, [q, q])
+    b.run(seeds)
+    for i, pb in enumerate(items):
+        occ, fit = b.read(i)
+        pocc, pfit, _ = hb.search(pb, q["num_solutions"], q["total_iter"], q["parallel_task"], q["converge_depth"],
+                                  seed=seeds[i])
+        np.testing.assert_array_equal(occ, pocc, err_msg=f"structure {i}")
+        np.testing.assert_array_equal(fit, pfit, err_msg=f"structure {i}")
+    b.close()
