@@ -4,19 +4,20 @@
 // Same contract as hea_search.cuh (Philox streams, counts, fitness order,
 // ties), so results are bit-identical to the shared-memory path; only where
 // the occupancy lives and how many SMs work on one solution change:
-//   * the occupancy row stays in HBM as 5*species bytes (converted in place at
-//     the start of a local search and back at the end), read through L1;
+//   * the occupancy row stays in HBM as species bytes; the local search does
+//     not read or write it: its draws take the species from the site
+//     histograms' species words (hist[s].w = 5*species), which the accepts
+//     keep current, and at its end each CTA writes its share of the row back
+//     from those words;
 //   * one thread-block cluster per solution: the round's tasks are split over
 //     the cluster's CTAs; each CTA reduces its warps' records, publishes its
 //     best in shared memory, and after one cluster barrier every warp reads the
 //     CL records through distributed shared memory and applies the same winner;
-//   * every CTA writes the accepted swap's two bytes itself, so a CTA's L1
-//     never holds a stale copy of its solution's row (the only writes to the
-//     row during the search are those swaps);
 //   * generation and recount are grid-wide over sites (many CTAs per solution);
 //     the recount also writes the site histograms the search scores from
 //     (hist, see score_delta), which rank 0 of the cluster updates after every
-//     accepted swap, followed by a cluster barrier.
+//     accepted swap, followed by a cluster barrier that only rank 0 arrives at
+//     with release semantics (the other CTAs have nothing to publish).
 #pragma once
 #include <cooperative_groups.h>
 
@@ -152,7 +153,6 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
     const int part = (n + csize - 1) / csize, lo = rank * part, hi = min(n, lo + part);
     const int qpart = (g.tasks + csize - 1) / csize, qlo = rank * qpart, qhi = min(g.tasks, qlo + qpart);
 
-    for (int s = lo + tid; s < hi; s += blockDim.x) row[s] = (uint8_t)(5 * row[s]);
     for (int x = tid; x < NC; x += blockDim.x) cnt2[x] = gcnt[x];
     __syncthreads();
     search_setup<T, S>(c, cnt2, tab);
@@ -233,8 +233,6 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
             const int xr = __ffs(__ballot_sync(0xFFFFFFFFu, own_k == xk && own_q == xq)) - 1;
             const SwapRecord w = *cluster.map_shared_rank(&cta_rec[round & 1], xr);
             const int a = w.ab & 0xFF, b = (w.ab >> 8) & 0xFF;
-            row[w.s1] = (uint8_t)(5 * b);  // every CTA writes the swap itself
-            row[w.s2] = (uint8_t)(5 * a);
             const int32_t *cold = cnt2 + buf * NCP;
             int32_t *cnew = cnt2 + (buf ^ 1) * NCP;
             const auto after = [cold, &w, a, b](int k, int i, int j) {
@@ -246,7 +244,14 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
             if (rank == 0)
                 update_hist<L, true>(c, g.nbor, hist, w.s1, w.s2, a, b,
                                      block_rotation(32 * (accept_linear_warps<T, S>() + (NC + 31) / 32)));
-            cluster.sync();  // the cluster's next proposals read the updated histograms; each CTA its table
+            // the cluster's next proposals read the histograms and species words rank 0 updated: rank 0
+            // arrives with release semantics, the others (whose accept work stays in their own shared
+            // memory) relaxed, every thread waits with acquire semantics.  Measured: 4 % per round.
+            if (rank == 0)
+                asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+            else
+                asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+            asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
             buf ^= 1;
             cur = __dadd_rn(cur, key_delta(xk));
             if (g.trace && rank == 0 && warp == 0 && accepts < g.trace_cap) {
@@ -271,8 +276,8 @@ __global__ void __launch_bounds__(512, 2) mc_large_kernel(const SearchConst c, c
         }
         ++round;
     }
-    cluster.sync();  // every CTA's last reads of the row are done
-    for (int s = lo + tid; s < hi; s += blockDim.x) row[s] = (uint8_t)(row[s] / 5);
+    cluster.sync();  // rank 0's last species words are visible
+    for (int s = lo + tid; s < hi; s += blockDim.x) row[s] = (uint8_t)(__ldcg(&hist[s].w) / 5u);
     if (rank == 0)
         for (int x = tid; x < NC; x += blockDim.x) gcnt[x] = cnt2[buf * NCP + x];
     unsigned long long ev = (unsigned long long)evals;
