@@ -4,7 +4,9 @@ Solutions and structures are independent (the reference splits solutions
 over MPI ranks, pyhea/cpp/accelerate.cpp:728, and gathers them on rank 0,
 pyhea/model/opt.py:73-80), so N GPUs run N independent replicas: each rank
 searches with its own seeds, and only the timing and counters are combined --
-there is no collective on the data path.
+there is no collective on the data path.  A batch of structures can instead
+be split across ranks (shard): each rank searches its share with the seeds
+the structures have in the whole batch.
 """
 import torch
 
@@ -12,6 +14,21 @@ import torch
 def replica_seed(rank, index, stride=1_000_003):
     """Seed of the index-th search of a rank; disjoint across ranks."""
     return stride * int(rank) + int(index)
+
+
+def shard(work, rank, world):
+    """Indices of the items rank `rank` of `world` searches: items taken in
+    descending work (ties by index) and each given to the rank with the least
+    work so far (lowest rank on ties).  Deterministic, the same on every rank;
+    every item goes to exactly one rank."""
+    load = [0.0] * int(world)
+    mine = []
+    for i in sorted(range(len(work)), key=lambda i: (-float(work[i]), i)):
+        r = min(range(int(world)), key=lambda r: (load[r], r))
+        load[r] += float(work[i])
+        if r == int(rank):
+            mine.append(i)
+    return sorted(mine)
 
 
 def combine(local_ms, local_evals, group=None, device=None):

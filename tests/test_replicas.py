@@ -51,3 +51,15 @@ def test_single_process_passthrough():
     assert replicas.combine(12.5, 7) == (12.5, 7.0)
     f, o = replicas.gather_best([0.3, 0.1], [[1], [2]])
     assert f == [0.1, 0.3] and o == [[2], [1]]
+
+
+def test_shard_partitions_every_item_once_and_balances_work():
+    work = [5, 1, 1, 1, 1, 1, 3, 2, 8, 2]
+    for world in (1, 2, 3, 4, 8):
+        parts = [replicas.shard(work, r, world) for r in range(world)]
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(work)))
+        loads = [sum(work[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(work)
+    assert replicas.shard(work, 0, 2) == replicas.shard(list(work), 0, 2)  # deterministic
+    assert replicas.shard([], 0, 4) == []
