@@ -138,12 +138,21 @@ py::tuple run_cuda(int nnet, int step, int task, int depth, double thr, const py
     }
     if (rc != HEA_OK) raise_for(rc);
 
+    // rows of Python ints built with the C API: one int object per species
+    // value (CPython's cached small ints), a new reference stored per element
+    std::vector<py::object> value(256);
+    for (int v = 0; v < 256; ++v) value[v] = py::int_(v);
     py::list latts(nnet);
     for (int p = 0; p < nnet; ++p) {
-        py::list row(N);
+        PyObject *row = PyList_New(N);
+        if (!row) throw py::error_already_set();
         const uint8_t *o = occ.data() + (size_t)p * N;
-        for (int s = 0; s < N; ++s) row[s] = py::int_(o[s]);
-        latts[p] = row;
+        for (int s = 0; s < N; ++s) {
+            PyObject *x = value[o[s]].ptr();
+            Py_INCREF(x);
+            PyList_SET_ITEM(row, s, x);  // steals the reference
+        }
+        latts[p] = py::reinterpret_steal<py::list>(row);
     }
     py::list fits(nnet);
     for (int p = 0; p < nnet; ++p) fits[p] = py::float_(fit[p]);
