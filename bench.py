@@ -309,6 +309,16 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # Batched: the mixed 64-structure batch
 # ---------------------------------------------------------------------------
+def neighbours_of(lattice_code, implicit):
+    """How a line's structures get their neighbours: described by the lattice, a table the library
+    recognised as an FCC/BCC cube's (both run on lattice arithmetic, same results), or a table."""
+    if implicit:
+        return "implicit (lattice arithmetic, no table)"
+    if lattice_code:
+        return "table, recognised as %s lattice's (lattice arithmetic, table not kept)" % ("an FCC", "a BCC")[lattice_code - 1]
+    return "table"
+
+
 def pinned_problem(pb):
     """The same problem with its host arrays in pinned memory (implicit problems keep no table)."""
     import numpy as np
@@ -349,6 +359,7 @@ def measure_batched(steps, warmup, l2_peak=None, implicit=False, select=None):
     batch.run(seeds(0))
     tuned = batch.autotune()  # launch configuration timed on full runs, before the warm-up
     plans = [hb.Plan(pb, st.P, st.I, st.Q, st.D, autotune=True) for pb, st in zip(problems, structs)]
+    recognised = all(plan.lattice for plan in plans)  # the batch builds its structures the same way
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for w in range(warmup):
         batch.run(seeds(w))
@@ -449,7 +460,7 @@ def measure_batched(steps, warmup, l2_peak=None, implicit=False, select=None):
                        "sites_total": int(sum(st.num_sites for st in structs)), "solutions": 64,
                        "parallel_task": 256, "total_iter": 10, "converge_depth": 10,
                        "l2": "flushed between timed steps (256 MiB write)", "batch_launch": tuned,
-                       "neighbours": "implicit (lattice arithmetic, no table)" if implicit else "table"},
+                       "neighbours": neighbours_of(1 if recognised else 0, implicit)},
             "plain": {"value": plain, "ms_per_step": p_ms / steps, "evals_per_step": p_ev / steps},
             "speedup_vs_plain": value / plain, "identical_structures": same, "structures": len(structs),
             "evals_per_step": b_ev / steps, "clocks": clocks, "roofline": roof,
@@ -536,6 +547,7 @@ def measure_large(iters, e2e=True, implicit=False):
     warm.run(0)
     warm.close()
     plan = hb.Plan(pb, st.P, iters, st.Q, st.D, time_kernels=True)
+    lattice_code = plan.lattice
     sampler = ClockSampler(torch.cuda.current_device()).start()
     s = plan.run(1)
     clocks = sampler.stop()
@@ -548,7 +560,7 @@ def measure_large(iters, e2e=True, implicit=False):
                       "parallel_task": st.Q, "converge_depth": st.D, "total_iter_run": iters,
                       "total_iter_stated": st.I, "max_rounds_per_local_search": None,
                       "warmup": "one capped (50-round) iteration",
-                      "neighbours": "implicit (lattice arithmetic, no table)" if implicit else "table",
+                      "neighbours": neighbours_of(lattice_code, implicit),
                       "l2": "inputs larger than L2 (4.1 GB of site histograms)"},
            "clocks": clocks}
     peak, peak_kind = measured_peaks()
@@ -870,6 +882,7 @@ def main():
     clocks = sampler.stop()
     _, best = plan.read()
     block = plan.local_search_block
+    lattice_code = plan.lattice
     plan.close()
 
     # end to end through the C ABI with pinned host buffers
@@ -906,7 +919,7 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(config_of(st, args.workload), parallelism=f"replicas x{world}",
-                           local_search_block=block),
+                           local_search_block=block, neighbours=neighbours_of(lattice_code, False)),
             # kernels launched per search: 1 generate + per iteration (generate, search, merge, search,
             # sort), plus the iota of the slot order
             "gpu_launches": args.steps * (2 + 5 * st.I),

@@ -52,10 +52,16 @@ typedef struct hea_problem {
      * always passes a table, lattice.py:196-323): with nbor == NULL, a perfect
      * FCC/BCC cube described here stands for the table, its neighbour ids are
      * computed on the device from lattice arithmetic and no table is stored.
-     * implicit_lattice: 1 FCC, 2 BCC (0: none, nbor required); lattice_cell:
-     * the cube's edge in unit cells (N = 4 or 2 cell^3); lattice_shell_set as in
-     * hea_build_neighbors.  shell_sizes must be the lattice's for the first S
-     * shells.  Results equal those with the table hea_build_neighbors builds. */
+     * implicit_lattice: 1 FCC, 2 BCC; lattice_cell: the cube's edge in unit
+     * cells (N = 4 or 2 cell^3); lattice_shell_set as in hea_build_neighbors.
+     * shell_sizes must be the lattice's for the first S shells.  Results equal
+     * those with the table hea_build_neighbors builds.
+     * With a table (nbor != NULL), implicit_lattice 0 lets the library
+     * recognise an FCC/BCC cube's table -- every shell of every site holding
+     * the ids hea_build_neighbors gives, in any order, as PyHEA's lattice
+     * tables do -- and run it on lattice arithmetic instead (same results; the
+     * table is not kept); -1 uses the table as given.  Plans report which form
+     * they run (hea_plan_lattice). */
     int32_t implicit_lattice;
     int32_t lattice_cell;
     int32_t lattice_shell_set;
@@ -139,6 +145,9 @@ int hea_plan_read(hea_plan *plan, uint8_t *out_occ, double *out_fitness);
 void hea_plan_destroy(hea_plan *plan);
 /* Threads per CTA of the plan's local search (the autotuner's pick with HEA_FLAG_AUTOTUNE). */
 int32_t hea_plan_local_search_block(const hea_plan *plan);
+/* Neighbours of the plan's structure: 0 from its table, 1 (FCC) or 2 (BCC)
+ * from lattice arithmetic (implicit, or a recognised lattice table). */
+int32_t hea_plan_lattice(const hea_plan *plan);
 
 /*
  * Batched search: `count` independent structures (each with its own problem,

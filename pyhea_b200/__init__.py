@@ -106,6 +106,7 @@ def _declare(lib):
         "hea_plan_read": (_i32, [ctypes.c_void_p, _P(_u8), _P(_f64)]),
         "hea_plan_destroy": (None, [ctypes.c_void_p]),
         "hea_plan_local_search_block": (_i32, [ctypes.c_void_p]),
+        "hea_plan_lattice": (_i32, [ctypes.c_void_p]),
         "hea_generate": (_i32, [_P(_Problem), _u64, _u32, _i32, _P(_u8), _P(_i32), _P(_f64)]),
         "hea_recount": (_i32, [_P(_Problem), _i32, _P(_u8), _P(_i32), _P(_f64)]),
         "hea_local_search": (_i32, [_P(_Problem), _u64, _u32, _i32, _i32, _i32, _i64, _P(_u8), _P(_i32), _P(_f64),
@@ -185,9 +186,12 @@ class Problem:
 
     ``Problem.from_lattice`` describes a perfect FCC/BCC cube instead of giving a
     table: the device computes neighbour ids from lattice arithmetic and stores
-    no table (same results as with the table ``build_neighbors`` makes)."""
+    no table (same results as with the table ``build_neighbors`` makes).  A
+    table that is such a cube's (every shell holding the lattice's ids, in any
+    order -- PyHEA's tables are) is recognised and run the same way unless
+    ``recognize=False``."""
 
-    def __init__(self, nbor, shell_sizes, species, weight, target_sro, lattice=None):
+    def __init__(self, nbor, shell_sizes, species, weight, target_sro, lattice=None, recognize=True):
         self.species = np.ascontiguousarray(species, dtype=np.int32)
         self.weight = np.ascontiguousarray(weight, dtype=np.float64)
         S, T = len(self.weight), len(self.species)
@@ -203,6 +207,8 @@ class Problem:
         self.num_types, self.num_shells = T, S
         self.lattice = lattice  # (FCC | BCC, cell, shell_set) of an implicit-neighbour problem, else None
         kind, cell, shell_set = (lattice[0] + 1, lattice[1], lattice[2]) if lattice is not None else (0, 0, 0)
+        if lattice is None and self.nbor is not None and not recognize:
+            kind = -1  # the table as given
         self._c = _Problem(self.num_sites, T, S, _ptr(self.shell_sizes, _i32), _ptr(self.nbor, _i32),
                            _ptr(self.species, _i32), _ptr(self.weight, _f64), _ptr(self.target_sro, _f64),
                            int(kind), int(cell), int(shell_set))
@@ -253,6 +259,12 @@ class Plan:
                  | (HEA_FLAG_AUTOTUNE if autotune else 0))
         prm = _params(num_solutions, total_iter, parallel_task, converge_depth, seed, max_rounds, flags)
         _check(_load().hea_plan_create(ctypes.byref(problem._c), ctypes.byref(prm), ctypes.byref(self._h)))
+
+    @property
+    def lattice(self):
+        """Neighbours the plan runs on: 0 its table, 1 FCC / 2 BCC lattice arithmetic (implicit, or a
+        recognised lattice table)."""
+        return int(_load().hea_plan_lattice(self._h))
 
     @property
     def local_search_block(self):

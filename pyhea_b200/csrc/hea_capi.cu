@@ -400,6 +400,51 @@ __global__ void build_neighbors_kernel(LatticeSpec sp, int L, int32_t *out, int 
     }
 }
 
+// Sets *mismatch unless the first S shells of every site's row in `raw`
+// ([N][raw_row], shells concatenated) hold the ids build_neighbors_kernel
+// gives for the lattice, in any order within a shell (both sides sorted
+// before the comparison).
+__global__ void lattice_match_kernel(LatticeSpec sp, int L, int S, const int32_t *raw, int raw_row, int *mismatch)
+{
+    const int n = sp.nb * L * L * L;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const int b = s % sp.nb, cell = s / sp.nb;
+        const int cx = cell / (L * L), cy = (cell / L) % L, cz = cell % L;
+        const int px = 2 * cx + sp.basis[b][0], py = 2 * cy + sp.basis[b][1], pz = 2 * cz + sp.basis[b][2];
+        const int32_t *o = raw + (size_t)s * raw_row;
+        bool same = true;
+        for (int k = 0; k < S && same; ++k) {
+            const int z = sp.size[k];
+            int ids[24], got[24];
+            for (int v = 0; v < z; ++v) {
+                const int qx = (px + sp.vec[k][v][0] + 2 * L) % (2 * L);
+                const int qy = (py + sp.vec[k][v][1] + 2 * L) % (2 * L);
+                const int qz = (pz + sp.vec[k][v][2] + 2 * L) % (2 * L);
+                ids[v] = sp.nb * ((qx >> 1) * L * L + (qy >> 1) * L + (qz >> 1)) + basis_of(sp, qx, qy, qz);
+                got[v] = o[v];
+            }
+            for (int i = 1; i < z; ++i) {  // insertion sorts, both sides
+                const int x = ids[i], y = got[i];
+                int j = i - 1;
+                while (j >= 0 && ids[j] > x) {
+                    ids[j + 1] = ids[j];
+                    --j;
+                }
+                ids[j + 1] = x;
+                j = i - 1;
+                while (j >= 0 && got[j] > y) {
+                    got[j + 1] = got[j];
+                    --j;
+                }
+                got[j + 1] = y;
+            }
+            for (int v = 0; v < z; ++v) same = same && ids[v] == got[v];
+            o += z;
+        }
+        if (!same) atomicOr(mismatch, 1);
+    }
+}
+
 int make_lattice_spec(int lattice, int shell_set, LatticeSpec &sp)
 {
     std::memset(&sp, 0, sizeof(sp));
@@ -655,6 +700,33 @@ uint32_t stream_histograms(size_t hist_bytes, size_t total_bytes)
     return hist_bytes > kSharedStreamBytes ? 1u : 0u;
 }
 
+// The FCC/BCC cube whose table `pb` may pass (implicit_lattice code 1 FCC,
+// 2 BCC; edge; shell set), from its site count and shell sizes alone; the
+// table itself is checked on the device (lattice_match_kernel).
+bool lattice_candidate(const hea_problem *pb, int &code, int &cell, int &shell_set)
+{
+    if (!pb->nbor || pb->implicit_lattice != 0) return false;
+    const int64_t n = pb->num_sites;
+    for (int lat = 0; lat < 2; ++lat) {
+        const int64_t nb = lat == 0 ? 4 : 2;
+        int64_t L = (int64_t)std::llround(std::cbrt((double)n / (double)nb));
+        if (L < 2 || L > 1024 || nb * L * L * L != n) continue;
+        for (int set = 0; set < (lat == 0 ? 2 : 1); ++set) {
+            LatticeSpec sp;
+            if (make_lattice_spec(lat, set, sp) != HEA_OK) continue;
+            bool fits = true;
+            for (int k = 0; k < pb->num_shells; ++k) fits = fits && pb->shell_sizes[k] == sp.size[k];
+            if (fits) {
+                code = lat + 1;
+                cell = (int)L;
+                shell_set = set;
+                return true;
+            }
+        }
+    }
+    return false;
+}
+
 int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t flags = 0)
 {
     HEA_TRY(validate_problem(pb));
@@ -667,6 +739,41 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t
     PadGeom g;
     fill_const(pb, seed, c, g);
     const int raw_row = g.raw_row, poff = g.pad_row;
+    const size_t raw_bytes = (size_t)N * raw_row * sizeof(int32_t);
+    struct Raw {  // the uploaded table, freed on every return
+        int32_t *p = nullptr;
+        ~Raw() { dev_free(p); }
+    } raw;
+
+    // a table that is an FCC/BCC cube's (PyHEA's lattice tables are) runs on lattice arithmetic
+    int code = 0, cell = 0, shell_set = 0;
+    if (lattice_candidate(pb, code, cell, shell_set)) {
+        LatticeSpec sp;
+        HEA_TRY(make_lattice_spec(code - 1, shell_set, sp));
+        struct Flag {
+            void *p = nullptr;
+            ~Flag() { dev_free(p); }
+        } flag;
+        int mismatch = 1;
+        if (dev_alloc(&raw.p, raw_bytes) != cudaSuccess || dev_alloc(&flag.p, sizeof(int)) != cudaSuccess)
+            return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes for the neighbour table", raw_bytes);
+        cudaError_t e = cudaMemcpy(raw.p, pb->nbor, raw_bytes, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(flag.p, 0, sizeof(int));
+        if (e == cudaSuccess) {
+            lattice_match_kernel<<<1184, 256>>>(sp, cell, S, raw.p, raw_row, static_cast<int *>(flag.p));
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaMemcpy(&mismatch, flag.p, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return fail(HEA_ERR_CUDA, "neighbour table upload failed: %s", cudaGetErrorString(e));
+        if (!mismatch) {
+            hea_problem q = *pb;
+            q.nbor = nullptr;
+            q.implicit_lattice = code;
+            q.lattice_cell = cell;
+            q.lattice_shell_set = shell_set;
+            fill_lattice_const(&q, c);
+        }
+    }
 
     // shared memory of the two kernels
     const size_t cnt_bytes = 4 * (size_t)((dt.ncount + 3) & ~3);
@@ -699,25 +806,22 @@ int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t
     }
 
     // padded table on the device, checked
-    const size_t raw_bytes = (size_t)N * raw_row * sizeof(int32_t);
     const size_t pad_bytes = (size_t)N * poff * sizeof(int32_t);
-    int32_t *raw = nullptr;
     int *derr = nullptr;
-    HEA_CUDA(dev_alloc(&raw, raw_bytes));
+    const bool uploaded = raw.p != nullptr;  // by the lattice check
+    if (!uploaded) HEA_CUDA(dev_alloc(&raw.p, raw_bytes));
     if (dev_alloc(&dt.nbor, pad_bytes) != cudaSuccess || dev_alloc(&derr, sizeof(int)) != cudaSuccess) {
-        dev_free(raw);
         dev_free(derr);
         return fail(HEA_ERR_NOMEM, "cannot allocate %zu bytes for the neighbour table", pad_bytes);
     }
     int herr = 0;
-    cudaError_t e = cudaMemcpy(raw, pb->nbor, raw_bytes, cudaMemcpyHostToDevice);
+    cudaError_t e = uploaded ? cudaSuccess : cudaMemcpy(raw.p, pb->nbor, raw_bytes, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(derr, 0, sizeof(int));
     if (e == cudaSuccess) {
-        pad_and_check_kernel<<<1184, 256>>>(raw, reinterpret_cast<int32_t *>(dt.nbor), g, derr);
+        pad_and_check_kernel<<<1184, 256>>>(raw.p, reinterpret_cast<int32_t *>(dt.nbor), g, derr);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost);
-    dev_free(raw);
     dev_free(derr);
     if (e != cudaSuccess) return fail(HEA_ERR_CUDA, "neighbour table upload failed: %s", cudaGetErrorString(e));
     if (herr & 1) return fail(HEA_ERR_INVALID, "neighbour list holds an id outside [0, %d)", N);
@@ -1346,6 +1450,12 @@ int hea_plan_read(hea_plan *plan, uint8_t *out_occ, double *out_fitness)
 void hea_plan_destroy(hea_plan *plan) { delete plan; }
 
 int32_t hea_plan_local_search_block(const hea_plan *plan) { return plan ? plan->mc_block : 0; }
+
+int32_t hea_plan_lattice(const hea_plan *plan)
+{
+    if (!plan || plan->dt.c.lat.L == 0) return 0;
+    return plan->dt.c.lat.kind == kLatBcc ? 2 : 1;
+}
 
 int hea_run_local_parallel_hcs(const hea_problem *problem, const hea_params *params, uint8_t *out_occ,
                                double *out_fitness, hea_stats *stats)

@@ -28,7 +28,7 @@ def pair(case, seed=0):
     lat, cell, species, shells, shell_set = case
     st = W.small_case(lattice=lat, cell=cell, species=species, shells=shells, shell_set=shell_set, seed=seed)
     nbor, sizes = hb.build_neighbors(lat, cell, shell_set)
-    table = hb.Problem(nbor, sizes, st.species, st.weight, st.target)
+    table = hb.Problem(nbor, sizes, st.species, st.weight, st.target, recognize=False)
     implicit = hb.Problem.from_lattice(lat, cell, st.species, st.weight, st.target, shell_set=shell_set)
     assert implicit.nbor is None
     return table, implicit
@@ -96,3 +96,40 @@ def test_server_lattice_requests_keep_no_table():
         np.testing.assert_array_equal(res[rid][0], res[r1][0])
         np.testing.assert_array_equal(res[rid][1], res[r1][1])
         assert res[rid][2]["device_bytes"] < res[r1][2]["device_bytes"]
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_lattice_tables_are_recognised(case):
+    """A lattice table, also with its shells' entries permuted, runs on lattice arithmetic with the
+    table's results; the same table with recognition off, or relabelled by a site permutation (a valid
+    table, not the lattice's), runs on the table."""
+    lat, cell, species, shells, shell_set = case
+    st = W.small_case(lattice=lat, cell=cell, species=species, shells=shells, shell_set=shell_set, seed=3)
+    nbor, sizes = hb.build_neighbors(lat, cell, shell_set)
+    nbor = nbor[:, : int(sizes[:shells].sum())]
+    rng = np.random.default_rng(0)
+    shuffled = nbor.copy()
+    off = np.concatenate([[0], np.cumsum(sizes[:shells])])
+    for k in range(shells):
+        seg = shuffled[:, off[k]:off[k + 1]]
+        shuffled[:, off[k]:off[k + 1]] = np.take_along_axis(seg, rng.permuted(np.tile(np.arange(seg.shape[1]), (len(seg), 1)), axis=1), axis=1)
+    perm = rng.permutation(len(nbor)).astype(np.int32)  # site s of the new labels is perm[s] of the old
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(len(perm), dtype=np.int32)
+    relabelled = inv[nbor[perm]]
+    q = dict(num_solutions=4, total_iter=2, parallel_task=48, converge_depth=3)
+    want = None
+    for table, recognize, lattice in ((nbor, False, 0), (nbor, True, lat + 1), (shuffled, True, lat + 1),
+                                      (relabelled, True, 0)):
+        pb = hb.Problem(table, sizes, st.species, st.weight, st.target, recognize=recognize)
+        plan = hb.Plan(pb, q["num_solutions"], q["total_iter"], q["parallel_task"], q["converge_depth"])
+        assert plan.lattice == lattice
+        plan.run(21)
+        got = plan.read()
+        plan.close()
+        if table is relabelled:
+            continue  # another labelling of the sites: other trajectories
+        if want is None:
+            want = got
+        np.testing.assert_array_equal(got[0], want[0])
+        np.testing.assert_array_equal(got[1], want[1])

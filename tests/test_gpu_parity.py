@@ -36,17 +36,20 @@ CASES = [
 FULL_SEARCH_CASES = CASES[:4] + CASES[6:]
 
 
-def pair(case, seed=0):
+def pair(case, seed=0, recognize=True):
+    """(library problem, oracle problem).  The cases' tables are lattice tables: with `recognize` the
+    library runs them on lattice arithmetic, without it on the table as given."""
     lat, cell, species, shells, shell_set = case
     st = W.small_case(lattice=lat, cell=cell, species=species, shells=shells, shell_set=shell_set, seed=seed)
     nbor, sizes = st.neighbors()
-    return (hb.Problem(nbor, sizes, st.species, st.weight, st.target),
+    return (hb.Problem(nbor, sizes, st.species, st.weight, st.target, recognize=recognize),
             ho.Problem(nbor[:, : int(sizes[:shells].sum())], sizes[:shells], st.species, st.weight, st.target))
 
 
+@pytest.mark.parametrize("recognize", [True, False])
 @pytest.mark.parametrize("case", CASES)
-def test_generate_bit_exact(case):
-    gp, op = pair(case)
+def test_generate_bit_exact(case, recognize):
+    gp, op = pair(case, recognize=recognize)
     occ, cnt, f2 = hb.generate(gp, seed=1234, generation=3, count=5)
     for s in range(5):
         want = op.generate(1234, 3, s)
@@ -69,11 +72,12 @@ def test_recount_matches_reference_engine(golden_engine, golden_nbor):
             assert abs(np.sqrt(f2[p]) - case["fitness"][p]) <= 1e-12 * case["fitness"][p]
 
 
+@pytest.mark.parametrize("recognize", [True, False])
 @pytest.mark.parametrize("case", CASES)
 @pytest.mark.parametrize("tasks", [1, 37, 64, 600])
-def test_local_search_trajectory_bit_exact(case, tasks):
+def test_local_search_trajectory_bit_exact(case, tasks, recognize):
     """Every accepted swap (round, task, sites, f2) and the counts after it equal the oracle's."""
-    gp, op = pair(case)
+    gp, op = pair(case, recognize=recognize)
     count, depth, call = 3, 4, 7
     occ0 = np.stack([op.generate(99, 2, s) for s in range(count)])
     got = hb.local_search(gp, 99, call, occ0, tasks, depth, trace_cap=4096, trace_counts=True)
@@ -91,9 +95,10 @@ def test_local_search_trajectory_bit_exact(case, tasks):
         np.testing.assert_array_equal(got["counts"][s], op.recount(got["occ"][s]))
 
 
+@pytest.mark.parametrize("recognize", [True, False])
 @pytest.mark.parametrize("case", FULL_SEARCH_CASES)
-def test_full_search_bit_exact(case):
-    gp, op = pair(case)
+def test_full_search_bit_exact(case, recognize):
+    gp, op = pair(case, recognize=recognize)
     occ, fit, stats = hb.search(gp, num_solutions=4, total_iter=2, parallel_task=32, converge_depth=4, seed=77)
     wocc, wf2, wstats = op.hcs(77, 4, 2, 32, 4)
     np.testing.assert_array_equal(occ, wocc)
