@@ -75,18 +75,19 @@ HBM_FALLBACK_GBS = 6650.0
 #   l2     lts__t_sectors_srcunit_tex.sum x 32 B              -> roofline.l2_frac
 #   inst   smsp__inst_executed.sum (warp instructions)        -> roofline.issue_frac
 #   dram_read  dram__bytes_read.sum                           -> roofline.dram_random (batched)
-# mc_kernel<5, Shells<2,2,3>>: the first local-search launch of `python bench.py --case plain
-# --iters 1` (203.72 M evaluations): 72.86 MB + 92.45 MB DRAM, 434.05 M L2 sectors, 4.0537 G warp
-# instructions.  batch_kernel: the launch of `python bench.py --case batch --count 64 --iters 10`, the
-# bench's batch configuration (6268.46 M evaluations): 1192.25 GB + 63.38 GB DRAM, 75.461 G L2 sectors,
-# 177.27 G warp instructions.  dram_random_probe_kernel (hea_dram_random_probe over 4 GiB, 77.59 M
+# mc_kernel<5, ImplicitShells<3>> (the plain structure's table is recognised as a BCC lattice's): the
+# first local-search launch of `python bench.py --case plain --iters 1` (203.72 M evaluations):
+# 69.81 MB + 92.28 MB DRAM, 428.96 M L2 sectors, 3.9814 G warp instructions.  batch_kernel: the launch
+# of `python bench.py --case batch --count 64 --iters 10`, the bench's batch configuration (6268.46 M
+# evaluations, lattice tables recognised): 1189.72 GB + 81.32 GB DRAM, 68.43 G L2 sectors, 178.51 G
+# warp instructions.  dram_random_probe_kernel (hea_dram_random_probe over 4 GiB, 77.59 M
 # random 16-byte loads): 9.833 GB DRAM read, i.e. 126.7 B per load (each load fetches a 128-byte line).
 KERNEL_COUNTERS = {
-    "plain_gpu": {"dram": (72.86e6 + 92.45e6) / 203.72e6, "l2": 434.05e6 * 32.0 / 203.72e6,
-                  "inst": 4.0537e9 / 203.72e6,
+    "plain_gpu": {"dram": (69.81e6 + 92.28e6) / 203.72e6, "l2": 428.96e6 * 32.0 / 203.72e6,
+                  "inst": 3.9814e9 / 203.72e6,
                   "capture": "mc_kernel, first local-search launch of bench.py --case plain --iters 1"},
-    "batched": {"dram": (1192.25e9 + 63.38e9) / 6268.46e6, "l2": 75.461e9 * 32.0 / 6268.46e6,
-                "inst": 177.27e9 / 6268.46e6, "dram_read": 1192.25e9 / 6268.46e6,
+    "batched": {"dram": (1189.72e9 + 81.32e9) / 6268.46e6, "l2": 68.43e9 * 32.0 / 6268.46e6,
+                "inst": 178.51e9 / 6268.46e6, "dram_read": 1189.72e9 / 6268.46e6,
                 "capture": "batch_kernel, bench.py --case batch --count 64 --iters 10"},
 }
 DRAM_BYTES_PER_RANDOM_LOAD = 9.833e9 / 77.594624e6
