@@ -727,6 +727,48 @@ bool lattice_candidate(const hea_problem *pb, int &code, int &cell, int &shell_s
     return false;
 }
 
+// Host twin of lattice_match_kernel, for the serving loop (which keeps a
+// request's table on the host until it is placed): every site's first S
+// shells of pb->nbor hold the lattice's ids, in any order within a shell.
+bool table_is_lattice(const hea_problem *pb, int code, int L, int shell_set)
+{
+    LatticeSpec sp;
+    if (make_lattice_spec(code - 1, shell_set, sp) != HEA_OK) return false;
+    const int S = pb->num_shells;
+    int row = 0;
+    for (int k = 0; k < S; ++k) row += pb->shell_sizes[k];
+    int basis_at[8];
+    for (int q = 0; q < 8; ++q) basis_at[q] = -1;
+    for (int b = 0; b < sp.nb; ++b)
+        basis_at[((sp.basis[b][0] & 1) << 2) | ((sp.basis[b][1] & 1) << 1) | (sp.basis[b][2] & 1)] = b;
+    std::vector<int32_t> ids, got;
+    const int64_t n = (int64_t)sp.nb * L * L * L;
+    for (int64_t s = 0; s < n; ++s) {
+        const int b = (int)(s % sp.nb);
+        const int64_t cell = s / sp.nb;
+        const int cx = (int)(cell / ((int64_t)L * L)), cy = (int)((cell / L) % L), cz = (int)(cell % L);
+        const int px = 2 * cx + sp.basis[b][0], py = 2 * cy + sp.basis[b][1], pz = 2 * cz + sp.basis[b][2];
+        const int32_t *o = pb->nbor + (size_t)s * row;
+        for (int k = 0; k < S; ++k) {
+            const int z = sp.size[k];
+            ids.resize(z);
+            got.assign(o, o + z);
+            for (int v = 0; v < z; ++v) {
+                const int qx = (px + sp.vec[k][v][0] + 2 * L) % (2 * L);
+                const int qy = (py + sp.vec[k][v][1] + 2 * L) % (2 * L);
+                const int qz = (pz + sp.vec[k][v][2] + 2 * L) % (2 * L);
+                ids[v] = (int32_t)(sp.nb * (((int64_t)(qx >> 1) * L + (qy >> 1)) * L + (qz >> 1)) +
+                                   basis_at[((qx & 1) << 2) | ((qy & 1) << 1) | (qz & 1)]);
+            }
+            std::sort(ids.begin(), ids.end());
+            std::sort(got.begin(), got.end());
+            if (ids != got) return false;
+            o += z;
+        }
+    }
+    return true;
+}
+
 int build_tables(const hea_problem *pb, uint64_t seed, DeviceTables &dt, int32_t flags = 0)
 {
     HEA_TRY(validate_problem(pb));
@@ -2792,7 +2834,14 @@ int hea_server_submit(hea_server *server, const hea_problem *problem, const hea_
     r.species.assign(problem->species, problem->species + r.T);
     r.weight.assign(problem->weight, problem->weight + r.S);
     r.target.assign(problem->target_sro, problem->target_sro + (size_t)r.S * r.T * r.T);
-    if (problem->nbor) {
+    int code = 0, cell = 0, shell_set = 0;
+    if (problem->nbor && lattice_candidate(problem, code, cell, shell_set) &&
+        table_is_lattice(problem, code, cell, shell_set)) {
+        // an FCC/BCC cube's table: the request runs on lattice arithmetic, as a lattice request
+        r.lattice = code - 1;
+        r.cell = cell;
+        r.shell_set = shell_set;
+    } else if (problem->nbor) {
         int64_t row = 0;
         for (int k = 0; k < r.S; ++k) row += r.shell_sizes[k];
         r.nbor.assign(problem->nbor, problem->nbor + (size_t)r.N * row);

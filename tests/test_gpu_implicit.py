@@ -133,3 +133,27 @@ def test_lattice_tables_are_recognised(case):
             want = got
         np.testing.assert_array_equal(got[0], want[0])
         np.testing.assert_array_equal(got[1], want[1])
+
+
+def test_server_recognises_lattice_tables():
+    """A lattice table submitted to the server runs as a lattice request: same result as the table
+    as given, and no table in the arena."""
+    case = (L.BCC, 5, (50, 50, 50, 50, 50), 3, L.SHELLS_REFERENCE)
+    tp, _ = pair(case)
+    rp = hb.Problem(tp.nbor, tp.shell_sizes, tp.species, tp.weight, tp.target_sro)  # recognised
+    q = dict(num_solutions=4, total_iter=2, parallel_task=64, converge_depth=3, seed=5)
+    srv = hb.Server(max_requests=4, slice_ms=20.0)
+    ids = [srv.submit(tp, q), srv.submit(rp, q)]
+    res = {}
+    while len(res) < 2:
+        srv.step()
+        for rid in ids:
+            if rid not in res:
+                got = srv.result(rid)
+                if got is not None:
+                    res[rid] = got
+    srv.close()
+    a, b = res[ids[0]], res[ids[1]]
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    assert b[2]["device_bytes"] < a[2]["device_bytes"]
